@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Benchmark: RK4 site-updates/s of the 256^3 droplet quench (real-time LHY RK4).
+
+Workload (precision config): LHY droplet, N = 5000, box [-L/2, L/2]^3 with L = 4 N^{1/3},
+256^3 grid, cubic coefficient quenched to -3.3, quartic 5/2, real-time RK4, dt = 5e-5.
+Start: Gaussian of width 0.5 N^{1/3} with seeded phase noise 1e-3 (synthetic, seed 2024);
+the step's cost does not depend on the state.  One step = one full RK4 step (4 stages).
+
+  value     site-updates/s, complex128, state resident in HBM (fields of 256 MiB >> L2, so
+            no flush is needed between steps)
+  fp32      the same in complex64 with FP64 reductions
+  e2e       the same metric through the host-buffer entry point: every step uploads the
+            state from pinned host memory, steps once, and downloads the result
+  roofline  dominant kernel of the step, algorithmic bytes / CUDA-event duration
+
+--impl reference times the CPU restatement of the reference's algorithm (oracle/, FFTs with
+all host threads) on the same workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 256
+N_ATOMS = 5000.0
+DT = 5e-5
+C3 = -3.3
+C4 = 2.5
+SEED = 2024
+
+# algorithmic field transfers (read + write, units of one field) of each launch of an RK4
+# step, in launch order: per stage x-fwd, y-fwd, z (fwd * K^2 * inv), y-inv, x-inv
+STAGE_XFWD = [2, 3, 3, 3]
+STAGE_XINV = [3, 5, 6, 5]
+KIND_NAMES = {0: "x_fwd_prologue", 10: "y_fwd", 22: "z_fwd_kinetic_inv", 11: "y_inv", 1: "x_inv_epilogue"}
+
+
+def workload_geometry():
+    L = 4.0 * N_ATOMS ** (1.0 / 3.0)
+    return (N_GRID,) * 3, (-L / 2,) * 3, (L / 2,) * 3
+
+
+def initial_state():
+    import numpy as np
+    from numpy.random import default_rng
+
+    shape, left, right = workload_geometry()
+    # Gaussian of width 0.5 N^{1/3}, phase noise 1e-3, normalised to N (host, numpy only)
+    sig = 0.5 * N_ATOMS ** (1.0 / 3.0)
+    x = [left[d] + (right[d] - left[d]) / shape[d] * (np.arange(shape[d]) + 0.5) for d in range(3)]
+    g = [np.exp(-xi * xi / (2 * sig * sig)) for xi in x]
+    psi = (g[0][:, None, None] * g[1][None, :, None] * g[2][None, None, :]).astype(np.complex128)
+    rng = default_rng(SEED)
+    psi *= np.exp(1j * 1e-3 * rng.uniform(-1, 1, psi.shape))
+    dV = 1.0
+    for d in range(3):
+        dV *= (right[d] - left[d]) / shape[d]
+    psi *= math.sqrt(N_ATOMS / (float(np.sum(np.abs(psi) ** 2)) * dV))
+    return np.asfortranarray(psi[..., None])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kind_name: str):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        v = d.get(kind_name)
+        if isinstance(v, dict):
+            return v.get("bytes_per_launch_256cubed")
+    return None
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from gp5_b200 import _abi
+
+    torch.cuda.set_device(local_rank)
+    dev = local_rank
+    shape, left, right = workload_geometry()
+    psi0 = initial_state()
+    sites = N_GRID ** 3
+    stream = torch.cuda.Stream(device=dev)
+    results = {}
+    launches = 0
+    for prec in (_abi.GP5_C128, _abi.GP5_C64):
+        plan = _abi.Plan(shape, left, right, precision=prec, device=dev)
+        plan.set_stream(stream.cuda_stream)
+        func = _abi.Functional(plan, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
+        st = _abi.Stepper(func, DT, _abi.GP5_STEP_RK4, imaginary=False)
+        f = plan.field(psi0)
+        st.advance(f, args.warmup)  # builds the step graph; W untimed steps
+        with torch.cuda.stream(stream):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            with ClockSampler(dev) as clk:
+                e0.record(stream)
+                st.advance(f, args.steps)
+                e1.record(stream)
+                torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if world > 1:
+                t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                ms = float(t.item())
+        lps = st.launches_per_step
+        launches += lps * args.steps
+        r = {"ms": ms, "ms_per_step": ms / args.steps, "value": world * sites * args.steps / (ms / 1e3),
+             "clocks": clk.summary(), "launches_per_step": lps}
+        # per-launch durations of one step (CUDA events between launches, same stream)
+        prof = st.profile(f, nrep=3)
+        r["profile"] = prof
+        if prec == _abi.GP5_C128:
+            # end to end: pinned host state in, one step, result back, per step
+            host_in = torch.empty(plan.field_bytes, dtype=torch.uint8).pin_memory()
+            host_out = torch.empty(plan.field_bytes, dtype=torch.uint8).pin_memory()
+            host_in.numpy()[:] = np.frombuffer(np.asfortranarray(psi0).tobytes(order="F"), dtype=np.uint8)
+            n_e2e = max(3, min(args.steps, 20))
+            st.advance_host(host_in.numpy(), host_out.numpy(), 1)  # warm
+            with torch.cuda.stream(stream):
+                torch.cuda.synchronize()
+                if world > 1:
+                    torch.distributed.barrier()
+                e0.record(stream)
+                for _ in range(n_e2e):
+                    st.advance_host(host_in.numpy(), host_out.numpy(), 1)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ems = e0.elapsed_time(e1)
+                if world > 1:
+                    t = torch.tensor([ems], device=f"cuda:{dev}", dtype=torch.float64)
+                    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                    ems = float(t.item())
+            launches += lps * n_e2e
+            r["e2e"] = {"value": world * sites * n_e2e / (ems / 1e3), "unit": "site-updates/s",
+                        "h2d_bytes_per_step": plan.field_bytes, "d2h_bytes_per_step": plan.field_bytes,
+                        "steps": n_e2e, "ms_per_step": ems / n_e2e}
+            r["field_bytes"] = plan.field_bytes
+        results[prec] = r
+        del f, st, func, plan
+        torch.cuda.synchronize()
+    return results, launches
+
+
+def roofline(r):
+    """Dominant kernel (largest share of a step) with its algorithmic bytes per launch."""
+    prof = r["profile"]
+    F = r["field_bytes"]
+    if len(prof) != 20:
+        return None
+    bytes_per = []
+    for s in range(4):
+        bytes_per += [STAGE_XFWD[s] * F, 2 * F, 2 * F, 2 * F, STAGE_XINV[s] * F]
+    tot = {}
+    for (kind, ms), b in zip(prof, bytes_per):
+        t = tot.setdefault(kind, [0.0, 0.0, 0])
+        t[0] += ms
+        t[1] += b
+        t[2] += 1
+    step_ms = sum(ms for _, ms in prof)
+    kind, (ms, b, n) = max(tot.items(), key=lambda kv: kv[1][0])
+    peak, src = measured_peaks()
+    achieved = b / (ms / 1e3) / 1e9
+    name = KIND_NAMES.get(kind, str(kind))
+    traffic = ncu_traffic(name)
+    step_bytes = sum(bytes_per)
+    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "peak_source": src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "algorithmic_bytes_per_launch": b / n, "launches_per_step": n,
+            "share_of_step": round(ms / step_ms, 4),
+            "step": {"algorithmic_bytes": step_bytes, "bytes_per_site": step_bytes / N_GRID ** 3,
+                     "achieved": round(step_bytes / (step_ms / 1e3) / 1e9, 1),
+                     "frac": round(step_bytes / (step_ms / 1e3) / 1e9 / peak, 4)},
+            "per_kind_ms": {KIND_NAMES.get(k, str(k)): round(v[0], 4) for k, v in tot.items()}}
+
+
+def cpu_reference_timing(max_seconds: float, max_steps: int, warm: bool = True):
+    """RK4 steps of the oracle (the reference's arithmetic) on the host, all threads."""
+    from oracle import gp_oracle as o
+
+    shape, left, right = workload_geometry()
+    geo = o.Geometry(shape, left, right)
+    psi = initial_state()
+    st = o.Stepper(o.Functional("lhy", c3=C3, c4=C4), geo, DT, "RK4", imaginary=False)
+    if warm:
+        psi = st.advance(psi, 1)
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps:
+        psi = st.advance(psi, 1)
+        n += 1
+        if time.perf_counter() - t0 > max_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": N_GRID ** 3 * n / dt, "unit": "site-updates/s", "cores": o._WORKERS, "kind": "port",
+            "steps": n, "seconds": dt,
+            "sample": f"{n} RK4 step(s) of the 256^3 complex128 workload; scipy.fft with "
+                      f"{o._WORKERS} workers, point-wise numpy on one thread"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": "LHY droplet quench, real-time RK4, 256^3, N=5000, L=4 N^(1/3), c3=-3.3, c4=2.5, "
+                          "dt=5e-5", "grid": [N_GRID] * 3, "precision_leg": ["complex128", "complex64"],
+              "l2": "inputs larger than L2 (each field 256 MiB)", "parallelism": f"replicas x{world}"}
+    metric = "RK4 site-updates/s at 256^3 (FP64; FP32 in 'fp32')"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        budget = 150.0
+        r = cpu_reference_timing(max_seconds=budget / max(1, args.steps) * args.steps, max_steps=args.steps,
+                                 warm=True)
+        line = {"impl": "reference", "metric": metric, "value": r["value"], "unit": "site-updates/s",
+                "n_gpus": args.gpus, "steps": r["steps"], "warmup": 1, "ms_per_step": r["seconds"] / r["steps"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": r["value"], "unit": "site-updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+        import datetime
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device(f"cuda:{local_rank}"))
+    results, launches = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    r64, r32 = results[0], results[1]
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        c = cpu_reference_timing(max_seconds=20.0, max_steps=4, warm=False)
+        cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    line = {"metric": metric, "value": r64["value"], "unit": "site-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r64["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic", "config": config,
+            "fp32": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "dtype": "c64",
+                     "speedup_vs_fp64": r32["value"] / r64["value"], "clocks": r32["clocks"],
+                     "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2))},
+            "e2e": r64["e2e"], "roofline": roofline(r64), "cpu_baseline": cpu,
+            "clocks": r64["clocks"], "gpu_launches": launches,
+            "launches_per_step": r64["launches_per_step"]}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

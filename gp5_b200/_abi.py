@@ -1,0 +1,349 @@
+"""ctypes binding of the C ABI in include/gp5cu.h, plus small owning wrappers.
+
+The wrappers (``Plan``, ``DeviceField``, ``Functional``, ``Stepper``) hold device memory
+allocated through the library itself, so no other GPU framework is needed.  Every call
+checks the status code and raises ``Gp5Error`` with the library's message; there is no
+fallback path: if ``libgp5cu.so`` is missing, importing this module fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgp5cu.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "gp5cu.h")
+
+GP5_OK, GP5_ERR_ARG, GP5_ERR_CUDA, GP5_ERR_NONFINITE, GP5_ERR_TIMEOUT = 0, 1, 2, 3, 4
+GP5_ERR_UNSUPPORTED, GP5_ERR_STATE, GP5_ERR_NOMEM = 5, 6, 7
+GP5_C128, GP5_C64 = 0, 1
+GP5_FORWARD, GP5_BACKWARD = -1, 1
+GP5_FUNC_GP, GP5_FUNC_LHY, GP5_FUNC_LHY_UNLOCKED = 0, 1, 2
+GP5_POT_NONE, GP5_POT_HARMONIC, GP5_POT_ARRAY = 0, 1, 2
+GP5_STEP_EULER, GP5_STEP_RK4 = 0, 1
+
+
+class Gp5Error(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"gp5cu status {status}: {msg}")
+        self.status = status
+
+
+class FunctionalDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("has_couplings", C.c_int),
+        ("couplings", C.c_double * 4),
+        ("masses", C.c_double * 2),
+        ("c3", C.c_double),
+        ("c4", C.c_double),
+        ("alpha", C.c_double),
+        ("beta", C.c_double),
+        ("eta", C.c_double),
+        ("potential", C.c_int),
+        ("omegas", (C.c_double * 3) * 2),
+        ("dpotential", C.c_void_p),
+    ]
+
+
+class Observables(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("norm", "energy", "ekin", "epot", "eint", "mu", "residual")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+def header_functions(path: str = HEADER):
+    """Names of every function declared in include/gp5cu.h."""
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(gp5cu_\w+)\s*\(", txt)))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built (python -m gp5_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    vp, i, d, pp = C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_void_p)
+    proto = {
+        "gp5cu_version": (i, []),
+        "gp5cu_status_string": (C.c_char_p, [i]),
+        "gp5cu_last_error": (C.c_char_p, []),
+        "gp5cu_plan_create": (i, [pp, C.POINTER(C.c_int), C.POINTER(d), C.POINTER(d), i, i, i]),
+        "gp5cu_plan_destroy": (i, [vp]),
+        "gp5cu_plan_set_stream": (i, [vp, vp]),
+        "gp5cu_plan_synchronize": (i, [vp]),
+        "gp5cu_field_bytes": (C.c_size_t, [vp]),
+        "gp5cu_field_alloc": (i, [vp, pp]),
+        "gp5cu_field_free": (i, [vp, vp]),
+        "gp5cu_upload": (i, [vp, vp, vp]),
+        "gp5cu_download": (i, [vp, vp, vp]),
+        "gp5cu_upload_c128": (i, [vp, vp, vp]),
+        "gp5cu_download_c128": (i, [vp, vp, vp]),
+        "gp5cu_fft": (i, [vp, vp, vp, i]),
+        "gp5cu_laplacian": (i, [vp, vp, vp]),
+        "gp5cu_norm": (i, [vp, vp, i, C.POINTER(d)]),
+        "gp5cu_normalize": (i, [vp, vp, i, d]),
+        "gp5cu_max_density": (i, [vp, vp, C.POINTER(d)]),
+        "gp5cu_functional_desc_init": (None, [C.POINTER(FunctionalDesc)]),
+        "gp5cu_functional_create": (i, [vp, C.POINTER(FunctionalDesc), pp]),
+        "gp5cu_functional_destroy": (i, [vp]),
+        "gp5cu_apply_H": (i, [vp, vp, vp]),
+        "gp5cu_observables": (i, [vp, vp, C.POINTER(Observables)]),
+        "gp5cu_stepper_create": (i, [vp, i, d, i, pp]),
+        "gp5cu_stepper_destroy": (i, [vp]),
+        "gp5cu_stepper_set_renormalization": (i, [vp, i, C.POINTER(d)]),
+        "gp5cu_stepper_set_phase_constraint": (i, [vp, vp]),
+        "gp5cu_stepper_advance": (i, [vp, vp, i]),
+        "gp5cu_stepper_get_time": (i, [vp, C.POINTER(d)]),
+        "gp5cu_stepper_set_time": (i, [vp, d]),
+        "gp5cu_stepper_advance_host": (i, [vp, vp, vp, i]),
+        "gp5cu_stepper_launches_per_step": (i, [vp]),
+        "gp5cu_stepper_profile": (i, [vp, vp, i, C.POINTER(d), C.POINTER(i), i, C.POINTER(i)]),
+    }
+    for name, (res, args) in proto.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != GP5_OK:
+        msg = lib().gp5cu_last_error().decode(errors="replace")
+        raise Gp5Error(status, msg)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Plan:
+    """Discretisation + FFT plan on one device (fourierTransformCreator::create)."""
+
+    def __init__(self, shape: Sequence[int], left: Sequence[float], right: Sequence[float],
+                 ncomp: int = 1, precision: int = GP5_C128, device: int = 0):
+        self.shape = tuple(int(s) for s in shape)
+        self.left = tuple(float(v) for v in left)
+        self.right = tuple(float(v) for v in right)
+        self.ncomp = int(ncomp)
+        self.precision = precision
+        h = C.c_void_p()
+        check(lib().gp5cu_plan_create(C.byref(h), (C.c_int * 3)(*self.shape), (C.c_double * 3)(*self.left),
+                                      (C.c_double * 3)(*self.right), self.ncomp, precision, device))
+        self.h = h
+
+    @property
+    def cdtype(self):
+        return np.complex128 if self.precision == GP5_C128 else np.complex64
+
+    @property
+    def field_shape(self):
+        return self.shape + (self.ncomp,)
+
+    @property
+    def field_bytes(self) -> int:
+        return int(lib().gp5cu_field_bytes(self.h))
+
+    def field(self, host: Optional[np.ndarray] = None) -> "DeviceField":
+        f = DeviceField(self)
+        if host is not None:
+            f.upload(host)
+        return f
+
+    def fft(self, src: "DeviceField", dst: "DeviceField", direction: int) -> None:
+        check(lib().gp5cu_fft(self.h, src.ptr, dst.ptr, direction))
+
+    def laplacian(self, src: "DeviceField", dst: "DeviceField") -> None:
+        check(lib().gp5cu_laplacian(self.h, src.ptr, dst.ptr))
+
+    def norm(self, f: "DeviceField", comp: int = 0) -> float:
+        out = C.c_double()
+        check(lib().gp5cu_norm(self.h, f.ptr, comp, C.byref(out)))
+        return out.value
+
+    def normalize(self, f: "DeviceField", N: float, comp: int = 0) -> None:
+        check(lib().gp5cu_normalize(self.h, f.ptr, comp, float(N)))
+
+    def max_density(self, f: "DeviceField") -> float:
+        out = C.c_double()
+        check(lib().gp5cu_max_density(self.h, f.ptr, C.byref(out)))
+        return out.value
+
+    def synchronize(self) -> None:
+        check(lib().gp5cu_plan_synchronize(self.h))
+
+    def set_stream(self, stream_handle: int) -> None:
+        check(lib().gp5cu_plan_set_stream(self.h, C.c_void_p(stream_handle or None)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gp5cu_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceField:
+    """One field (nx, ny, nz, ncomp) in device memory, allocated by the library."""
+
+    def __init__(self, plan: Plan):
+        self.plan = plan
+        p = C.c_void_p()
+        check(lib().gp5cu_field_alloc(plan.h, C.byref(p)))
+        self.ptr = p
+
+    def upload(self, host: np.ndarray) -> None:
+        a = np.asarray(host)
+        if a.ndim == 3:
+            a = a[..., None]
+        if a.shape != self.plan.field_shape:
+            raise ValueError(f"shape {a.shape} != {self.plan.field_shape}")
+        a = np.asfortranarray(a.astype(np.complex128, copy=False))
+        if self.plan.precision == GP5_C128:
+            check(lib().gp5cu_upload(self.plan.h, self.ptr, C.c_void_p(_ptr(a))))
+        else:
+            check(lib().gp5cu_upload_c128(self.plan.h, self.ptr, C.c_void_p(_ptr(a))))
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.plan.field_shape, dtype=np.complex128, order="F")
+        if self.plan.precision == GP5_C128:
+            check(lib().gp5cu_download(self.plan.h, self.ptr, C.c_void_p(_ptr(out))))
+        else:
+            check(lib().gp5cu_download_c128(self.plan.h, self.ptr, C.c_void_p(_ptr(out))))
+        return out
+
+    def close(self):
+        if getattr(self, "ptr", None) and getattr(self.plan, "h", None):
+            lib().gp5cu_field_free(self.plan.h, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Functional:
+    def __init__(self, plan: Plan, kind: int = GP5_FUNC_LHY, couplings=None, masses=None, c3=-3.0, c4=2.5,
+                 alpha=0.0, beta=0.0, eta=0.0, omegas=None, potential: Optional[DeviceField] = None,
+                 potential_ptr: Optional[int] = None):
+        self.plan = plan
+        d = FunctionalDesc()
+        lib().gp5cu_functional_desc_init(C.byref(d))
+        d.kind = kind
+        if couplings is not None:
+            g = np.asarray(couplings, dtype=np.float64).reshape(-1)
+            if g.size == 1:
+                d.couplings[0] = g[0]
+            else:
+                for k in range(4):
+                    d.couplings[k] = g[k]
+            d.has_couplings = 1
+        if masses is not None:
+            for c, m in enumerate(masses):
+                d.masses[c] = m
+        d.c3, d.c4, d.alpha, d.beta, d.eta = c3, c4, alpha, beta, eta
+        if omegas is not None:
+            d.potential = GP5_POT_HARMONIC
+            for c, w in enumerate(omegas):
+                for k in range(3):
+                    d.omegas[c][k] = w[k]
+        if potential_ptr is not None:
+            d.potential = GP5_POT_ARRAY
+            d.dpotential = potential_ptr
+        self.desc = d
+        h = C.c_void_p()
+        check(lib().gp5cu_functional_create(plan.h, C.byref(d), C.byref(h)))
+        self.h = h
+
+    def apply(self, src: DeviceField, dst: DeviceField) -> None:
+        check(lib().gp5cu_apply_H(self.h, src.ptr, dst.ptr))
+
+    def observables(self, f: DeviceField) -> dict:
+        o = Observables()
+        check(lib().gp5cu_observables(self.h, f.ptr, C.byref(o)))
+        return o.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gp5cu_functional_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Stepper:
+    def __init__(self, func: Functional, dt: float, kind: int = GP5_STEP_RK4, imaginary: bool = True):
+        self.func = func
+        self.dt = float(dt)
+        h = C.c_void_p()
+        check(lib().gp5cu_stepper_create(func.h, kind, self.dt, 1 if imaginary else 0, C.byref(h)))
+        self.h = h
+
+    def set_renormalization(self, N: Optional[Sequence[float]]) -> None:
+        if N is None:
+            check(lib().gp5cu_stepper_set_renormalization(self.h, 0, None))
+        else:
+            arr = (C.c_double * len(N))(*N)
+            check(lib().gp5cu_stepper_set_renormalization(self.h, len(N), arr))
+
+    def set_phase_constraint(self, phase: Optional[DeviceField]) -> None:
+        check(lib().gp5cu_stepper_set_phase_constraint(self.h, phase.ptr if phase is not None else None))
+
+    def advance(self, f: DeviceField, nsteps: int = 1) -> None:
+        check(lib().gp5cu_stepper_advance(self.h, f.ptr, int(nsteps)))
+
+    def advance_host(self, host_in: np.ndarray, host_out: np.ndarray, nsteps: int) -> None:
+        check(lib().gp5cu_stepper_advance_host(self.h, C.c_void_p(_ptr(host_in)), C.c_void_p(_ptr(host_out)),
+                                               int(nsteps)))
+
+    @property
+    def time(self) -> float:
+        t = C.c_double()
+        check(lib().gp5cu_stepper_get_time(self.h, C.byref(t)))
+        return t.value
+
+    def profile(self, f: DeviceField, nrep: int = 3):
+        """Mean duration (ms) and kind of every kernel launch of one step."""
+        cap = 256
+        ms = (C.c_double * cap)()
+        kinds = (C.c_int * cap)()
+        n = C.c_int()
+        check(lib().gp5cu_stepper_profile(self.h, f.ptr, int(nrep), ms, kinds, cap, C.byref(n)))
+        return [(int(kinds[k]), float(ms[k])) for k in range(min(n.value, cap))]
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(lib().gp5cu_stepper_launches_per_step(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gp5cu_stepper_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,54 @@
+// common.cuh - precision traits, complex helpers and small device utilities shared by the
+// sm_100a kernels of the GP stepper.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gp5 {
+
+// Complex element type per precision: double2 for complex128, float2 for complex64.
+template <typename R> struct CT;
+template <> struct CT<double> { using T = double2; };
+template <> struct CT<float> { using T = float2; };
+
+template <typename R> using cpx = typename CT<R>::T;
+
+template <typename R> __host__ __device__ __forceinline__ cpx<R> mk(R re, R im) {
+    cpx<R> v;
+    v.x = re;
+    v.y = im;
+    return v;
+}
+template <typename V> __host__ __device__ __forceinline__ V cadd(V a, V b) {
+    V r; r.x = a.x + b.x; r.y = a.y + b.y; return r;
+}
+template <typename V> __host__ __device__ __forceinline__ V csub(V a, V b) {
+    V r; r.x = a.x - b.x; r.y = a.y - b.y; return r;
+}
+// (a+ib)(c+id) = (ac - bd) + i(ad + bc), the order std::complex uses
+template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
+    V r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+// a * conj(b)
+template <typename V> __host__ __device__ __forceinline__ V cmulc(V a, V b) {
+    V r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
+}
+template <typename V, typename S> __host__ __device__ __forceinline__ V cscale(V a, S s) {
+    V r; r.x = a.x * s; r.y = a.y * s; return r;
+}
+// multiply by -i (DIR=-1) or +i (DIR=+1)
+template <int DIR, typename V> __host__ __device__ __forceinline__ V mul_i(V a) {
+    V r;
+    if (DIR < 0) { r.x = a.y; r.y = -a.x; }
+    else { r.x = -a.y; r.y = a.x; }
+    return r;
+}
+template <typename V> __host__ __device__ __forceinline__ V cconj(V a) {
+    V r; r.x = a.x; r.y = -a.y; return r;
+}
+
+// ---- status words shared with the host ------------------------------------------------
+enum DevStatus : unsigned { DS_OK = 0u, DS_NONFINITE = 1u, DS_TIMEOUT = 2u };
+
+}  // namespace gp5

@@ -1,0 +1,761 @@
+// gp5cu_host.cu - the C ABI (include/gp5cu.h): plans, functionals, steppers.
+//
+// Host logic only; the kernels and their launch sequences live in launch_impl.cuh.  Every
+// entry point catches the library's internal errors and returns a status code; the message
+// is kept per thread for gp5cu_last_error().
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace gp5 {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+[[noreturn]] void fail(int status, const std::string &msg) { throw Gp5Error{status, msg}; }
+
+void check_cuda(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        const int st = (e == cudaErrorMemoryAllocation) ? GP5_ERR_NOMEM : GP5_ERR_CUDA;
+        fail(st, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+__global__ void k_set_scalars(DevScalars *ds) {
+    ds->sigma[0] = ds->sigma[1] = 1.0;
+    ds->alpha[0] = ds->alpha[1] = 1.0;
+    ds->status = 0u;
+}
+
+void ProfRec::record(cudaStream_t s, int kind) {
+    if (idx >= ev.size()) {
+        cudaEvent_t e;
+        check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+        ev.push_back(e);
+        kinds.push_back(kind);
+    }
+    kinds[idx] = kind;
+    check_cuda(cudaEventRecord(ev[idx], s), "cudaEventRecord");
+    idx++;
+}
+
+void set_scalars(cudaStream_t s, DevScalars *ds) {
+    k_set_scalars<<<1, 1, 0, s>>>(ds);
+    check_cuda(cudaGetLastError(), "k_set_scalars");
+}
+
+// Factorisation into the radices of the shared-memory engine: 8 and 4 first, then 2, the
+// small odd primes with dedicated butterflies, then any remaining prime up to 61.
+static bool factorize(int n, LineSchedule &s) {
+    s.n = n;
+    s.np = 0;
+    int m = n;
+    auto push = [&](int r) {
+        if (s.np >= kMaxPasses) return false;
+        s.rad[s.np++] = r;
+        m /= r;
+        return true;
+    };
+    while (m % 8 == 0) if (!push(8)) return false;
+    while (m % 4 == 0) if (!push(4)) return false;
+    while (m % 2 == 0) if (!push(2)) return false;
+    while (m % 3 == 0) if (!push(3)) return false;
+    while (m % 5 == 0) if (!push(5)) return false;
+    for (int p = 7; p < kMaxRadix && m > 1; p += 2) {
+        while (m % p == 0) if (!push(p)) return false;
+    }
+    return m == 1;
+}
+
+template <typename Real> static void *upload_twiddles(int n) {
+    std::vector<cpx<Real>> h(n);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int j = 0; j < n; j++) {
+        const long double a = twopi * (long double)j / (long double)n;
+        h[j] = mk<Real>((Real)cosl(a), (Real)(-sinl(a)));
+    }
+    void *d = nullptr;
+    check_cuda(cudaMalloc(&d, sizeof(cpx<Real>) * n), "cudaMalloc twiddles");
+    check_cuda(cudaMemcpy(d, h.data(), sizeof(cpx<Real>) * n, cudaMemcpyHostToDevice), "upload twiddles");
+    return d;
+}
+
+void build_axis_plan(gp5cu_plan *p, int d) {
+    AxisPlan &ap = p->ax[d];
+    const int n = p->shape[d];
+    ap.n = n;
+    ap.reg = (n == 32 || n == 64 || n == 128 || n == 256 || n == 512);
+    if (!factorize(n, ap.sched))
+        fail(GP5_ERR_UNSUPPORTED, "axis length " + std::to_string(n) + " has a prime factor > 61");
+    ap.tw = p->prec == GP5_C128 ? upload_twiddles<double>(n) : upload_twiddles<float>(n);
+    const size_t eb = p->elem_bytes;
+    const size_t budget = 96 * 1024;
+    long long lines = (long long)(budget / (2 * (size_t)(n + 1) * eb));
+    if (lines < 1) {
+        lines = 1;
+        if (2 * (size_t)(n + 1) * eb > 200 * 1024)
+            fail(GP5_ERR_UNSUPPORTED, "axis length " + std::to_string(n) + " too long for one tile");
+    }
+    ap.smem_lines = (int)std::min<long long>(lines, 64);
+}
+
+}  // namespace gp5
+
+using namespace gp5;
+
+// ---------------------------------------------------------------------------------------------
+#define GP5_TRY try {
+#define GP5_CATCH                                  \
+    }                                              \
+    catch (const Gp5Error &e) {                    \
+        set_last_error(e.msg);                     \
+        return e.status;                           \
+    }                                              \
+    catch (const std::exception &e) {              \
+        set_last_error(e.what());                  \
+        return GP5_ERR_ARG;                        \
+    }                                              \
+    return GP5_OK;
+
+static void use_device(const gp5cu_plan *p) { check_cuda(cudaSetDevice(p->dev), "cudaSetDevice"); }
+
+static void require(bool cond, const std::string &msg) {
+    if (!cond) fail(GP5_ERR_ARG, msg);
+}
+
+static void check_field_ptr(const void *ptr, const char *name) {
+    require(ptr != nullptr, std::string(name) + " is NULL");
+    require(((uintptr_t)ptr & 15u) == 0, std::string(name) + " is not 16-byte aligned");
+}
+
+static void sync_and_check(gp5cu_plan *p, DevScalars *ds) {
+    check_cuda(cudaStreamSynchronize(p->stream), "cudaStreamSynchronize");
+    if (ds) {
+        unsigned st = 0;
+        check_cuda(cudaMemcpy(&st, &ds->status, sizeof(unsigned), cudaMemcpyDeviceToHost), "read status");
+        if (st & DS_NONFINITE) fail(GP5_ERR_NONFINITE, "a reduction met NaN/Inf (norm blow-up)");
+        if (st & DS_TIMEOUT) fail(GP5_ERR_TIMEOUT, "a bounded device wait ran out");
+    }
+}
+
+template <class F> static void dispatch(const gp5cu_plan *p, F &&f) {
+    if (p->prec == GP5_C128) f((double)0);
+    else f((float)0);
+}
+
+extern "C" {
+
+int gp5cu_version(void) { return 10000; }
+
+const char *gp5cu_status_string(int status) {
+    switch (status) {
+        case GP5_OK: return "ok";
+        case GP5_ERR_ARG: return "invalid argument";
+        case GP5_ERR_CUDA: return "CUDA error";
+        case GP5_ERR_NONFINITE: return "non-finite value in a reduction";
+        case GP5_ERR_TIMEOUT: return "device wait timed out";
+        case GP5_ERR_UNSUPPORTED: return "unsupported";
+        case GP5_ERR_STATE: return "invalid state";
+        case GP5_ERR_NOMEM: return "out of device memory";
+        default: return "unknown status";
+    }
+}
+
+const char *gp5cu_last_error(void) { return g_last_error.c_str(); }
+
+int gp5cu_plan_create(gp5cu_plan **out, const int shape[3], const double left[3], const double right[3],
+                      int ncomp, int precision, int device) {
+    GP5_TRY
+    require(out != nullptr, "out is NULL");
+    *out = nullptr;
+    require(shape && left && right, "shape/left/right must not be NULL");
+    require(ncomp == 1 || ncomp == 2, "ncomp must be 1 or 2");
+    require(precision == GP5_C128 || precision == GP5_C64, "precision must be GP5_C128 or GP5_C64");
+    for (int d = 0; d < 3; d++) {
+        require(shape[d] >= 2 && shape[d] <= 4096, "each axis length must be in [2, 4096]");
+        require(right[d] > left[d], "domain right must exceed left on every axis");
+    }
+    int ndev = 0;
+    check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    require(device >= 0 && device < ndev, "device ordinal out of range");
+    gp5cu_plan *p = new gp5cu_plan();
+    try {
+        p->dev = device;
+        use_device(p);
+        for (int d = 0; d < 3; d++) {
+            p->shape[d] = shape[d];
+            p->left[d] = left[d];
+            p->right[d] = right[d];
+        }
+        p->ncomp = ncomp;
+        p->prec = precision;
+        p->nsites = (long long)shape[0] * shape[1] * shape[2];
+        p->elem_bytes = precision == GP5_C128 ? 16 : 8;
+        p->field_bytes = (size_t)p->nsites * ncomp * p->elem_bytes;
+        // dV = product of space steps in axis order (geometry.cpp:206-210)
+        double dv = 1.0;
+        for (int d = 0; d < 3; d++) dv *= (right[d] - left[d]) / shape[d];
+        p->dV = dv;
+        check_cuda(cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        p->stream = p->own_stream;
+        for (int d = 0; d < 3; d++) {
+            build_axis_plan(p, d);
+            // k_d = (2 pi / L) m, m = i (i < n/2, even n; i <= (n-1)/2, odd n) else i - n
+            // (geometry.cpp:108-152); tabulated squared, as K*K in operators.cpp:20.
+            const int n = shape[d];
+            const double delta = 2 * M_PI / (right[d] - left[d]);
+            std::vector<double> k2(n);
+            p->pos_host[d].resize(n);
+            const double dx = (right[d] - left[d]) / n;
+            for (int i = 0; i < n; i++) {
+                double k;
+                if (n % 2 == 0) k = (i < n / 2) ? delta * i : (-n + i) * delta;
+                else k = (i <= (n - 1) / 2) ? delta * i : (-n + i) * delta;
+                k2[i] = k * k;
+                p->pos_host[d][i] = left[d] + dx * (i + 0.5);  // geometry.cpp:184
+            }
+            check_cuda(cudaMalloc(&p->k2[d], sizeof(double) * n), "cudaMalloc k2");
+            check_cuda(cudaMemcpy(p->k2[d], k2.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload k2");
+        }
+        check_cuda(cudaMalloc(&p->work, p->field_bytes), "cudaMalloc work");
+        // partial-sum slots: the largest grid any kernel of this plan launches
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        p->pw_blocks = sms * 8;
+        long long mb = p->pw_blocks;
+        for (int d = 0; d < 3; d++) {
+            const int lines_reg = 256 / (p->shape[d] <= 64 ? 8 : (p->shape[d] == 512 ? 64 : 16));
+            const int lines = std::min(lines_reg, p->ax[d].smem_lines);
+            // worst case: one line per tile
+            long long lines_total = d == 0 ? (long long)shape[1] * shape[2] * ncomp
+                                           : (d == 1 ? (long long)shape[0] * shape[2] * ncomp
+                                                     : (long long)shape[0] * shape[1] * ncomp);
+            (void)lines;
+            mb = std::max(mb, lines_total);
+        }
+        p->max_blocks = mb;
+        check_cuda(cudaMalloc(&p->partials, sizeof(double) * kNRed * mb), "cudaMalloc partials");
+        check_cuda(cudaMalloc(&p->counter, sizeof(unsigned)), "cudaMalloc counter");
+        check_cuda(cudaMemset(p->counter, 0, sizeof(unsigned)), "memset counter");
+        check_cuda(cudaMalloc(&p->ds, sizeof(DevScalars)), "cudaMalloc scalars");
+        check_cuda(cudaMemset(p->ds, 0, sizeof(DevScalars)), "memset scalars");
+        check_cuda(cudaMalloc(&p->dmax, sizeof(unsigned long long)), "cudaMalloc dmax");
+        set_scalars(p->stream, p->ds);
+        check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    } catch (...) {
+        gp5cu_plan_destroy(p);
+        throw;
+    }
+    *out = p;
+    GP5_CATCH
+}
+
+int gp5cu_plan_destroy(gp5cu_plan *p) {
+    if (!p) return GP5_OK;
+    cudaSetDevice(p->dev);
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    for (int d = 0; d < 3; d++) {
+        cudaFree(p->ax[d].tw);
+        cudaFree(p->k2[d]);
+    }
+    cudaFree(p->work);
+    cudaFree(p->partials);
+    cudaFree(p->counter);
+    cudaFree(p->ds);
+    cudaFree(p->dmax);
+    if (p->own_stream) cudaStreamDestroy(p->own_stream);
+    delete p;
+    return GP5_OK;
+}
+
+int gp5cu_plan_set_stream(gp5cu_plan *p, void *stream) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    use_device(p);
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+    GP5_CATCH
+}
+
+int gp5cu_plan_synchronize(gp5cu_plan *p) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    use_device(p);
+    check_cuda(cudaStreamSynchronize(p->stream), "cudaStreamSynchronize");
+    GP5_CATCH
+}
+
+size_t gp5cu_field_bytes(const gp5cu_plan *p) { return p ? p->field_bytes : 0; }
+
+int gp5cu_field_alloc(gp5cu_plan *p, void **dfield) {
+    GP5_TRY
+    require(p && dfield, "NULL argument");
+    use_device(p);
+    *dfield = nullptr;
+    check_cuda(cudaMalloc(dfield, p->field_bytes), "cudaMalloc field");
+    check_cuda(cudaMemsetAsync(*dfield, 0, p->field_bytes, p->stream), "memset field");
+    GP5_CATCH
+}
+
+int gp5cu_field_free(gp5cu_plan *p, void *dfield) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    use_device(p);
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    check_cuda(cudaFree(dfield), "cudaFree");
+    GP5_CATCH
+}
+
+int gp5cu_upload(gp5cu_plan *p, void *dfield, const void *host) {
+    GP5_TRY
+    require(p && host, "NULL argument");
+    check_field_ptr(dfield, "dfield");
+    use_device(p);
+    check_cuda(cudaMemcpyAsync(dfield, host, p->field_bytes, cudaMemcpyHostToDevice, p->stream), "upload");
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    GP5_CATCH
+}
+
+int gp5cu_download(gp5cu_plan *p, const void *dfield, void *host) {
+    GP5_TRY
+    require(p && host, "NULL argument");
+    check_field_ptr(dfield, "dfield");
+    use_device(p);
+    check_cuda(cudaMemcpyAsync(host, dfield, p->field_bytes, cudaMemcpyDeviceToHost, p->stream), "download");
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    GP5_CATCH
+}
+
+int gp5cu_upload_c128(gp5cu_plan *p, void *dfield, const double *host) {
+    GP5_TRY
+    require(p && host, "NULL argument");
+    check_field_ptr(dfield, "dfield");
+    use_device(p);
+    if (p->prec == GP5_C128) return gp5cu_upload(p, dfield, host);
+    const size_t n = (size_t)p->nsites * p->ncomp;
+    double *tmp = nullptr;
+    check_cuda(cudaMalloc(&tmp, n * 16), "cudaMalloc staging");
+    try {
+        check_cuda(cudaMemcpyAsync(tmp, host, n * 16, cudaMemcpyHostToDevice, p->stream), "upload");
+        Launch<float>::convert(p, tmp, dfield, nullptr, nullptr);
+        check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    } catch (...) {
+        cudaFree(tmp);
+        throw;
+    }
+    cudaFree(tmp);
+    GP5_CATCH
+}
+
+int gp5cu_download_c128(gp5cu_plan *p, const void *dfield, double *host) {
+    GP5_TRY
+    require(p && host, "NULL argument");
+    check_field_ptr(dfield, "dfield");
+    use_device(p);
+    if (p->prec == GP5_C128) return gp5cu_download(p, dfield, host);
+    const size_t n = (size_t)p->nsites * p->ncomp;
+    double *tmp = nullptr;
+    check_cuda(cudaMalloc(&tmp, n * 16), "cudaMalloc staging");
+    try {
+        Launch<float>::convert(p, nullptr, nullptr, dfield, tmp);
+        check_cuda(cudaMemcpyAsync(host, tmp, n * 16, cudaMemcpyDeviceToHost, p->stream), "download");
+        check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    } catch (...) {
+        cudaFree(tmp);
+        throw;
+    }
+    cudaFree(tmp);
+    GP5_CATCH
+}
+
+int gp5cu_fft(gp5cu_plan *p, const void *src, void *dst, int direction) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    check_field_ptr(src, "src");
+    check_field_ptr(dst, "dst");
+    require(direction == GP5_FORWARD || direction == GP5_BACKWARD, "direction must be GP5_FORWARD or GP5_BACKWARD");
+    use_device(p);
+    dispatch(p, [&](auto r) { Launch<decltype(r)>::fft(p, src, dst, direction); });
+    GP5_CATCH
+}
+
+int gp5cu_laplacian(gp5cu_plan *p, const void *src, void *dst) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    check_field_ptr(src, "src");
+    check_field_ptr(dst, "dst");
+    use_device(p);
+    dispatch(p, [&](auto r) { Launch<decltype(r)>::laplacian(p, src, dst); });
+    GP5_CATCH
+}
+
+int gp5cu_norm(gp5cu_plan *p, const void *field, int comp, double *out) {
+    GP5_TRY
+    require(p && out, "NULL argument");
+    check_field_ptr(field, "field");
+    require(comp >= 0 && comp < p->ncomp, "component out of range");
+    use_device(p);
+    dispatch(p, [&](auto r) { Launch<decltype(r)>::norm(p, field, comp, 0.0, p->ds); });
+    double s = 0;
+    check_cuda(cudaMemcpyAsync(&s, &p->ds->sums[0], sizeof(double), cudaMemcpyDeviceToHost, p->stream), "read");
+    sync_and_check(p, p->ds);
+    *out = s * p->dV;
+    GP5_CATCH
+}
+
+int gp5cu_normalize(gp5cu_plan *p, void *field, int comp, double N) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    check_field_ptr(field, "field");
+    require(comp >= 0 && comp < p->ncomp, "component out of range");
+    require(N > 0, "normalisation must be positive");
+    use_device(p);
+    dispatch(p, [&](auto r) {
+        Launch<decltype(r)>::norm(p, field, comp, N, p->ds);
+        Launch<decltype(r)>::scale(p, field, comp, p->ds, false);
+    });
+    GP5_CATCH
+}
+
+int gp5cu_max_density(gp5cu_plan *p, const void *field, double *out) {
+    GP5_TRY
+    require(p && out, "NULL argument");
+    check_field_ptr(field, "field");
+    use_device(p);
+    dispatch(p, [&](auto r) { Launch<decltype(r)>::max_density(p, field); });
+    unsigned long long bits = 0;
+    check_cuda(cudaMemcpyAsync(&bits, p->dmax, sizeof(bits), cudaMemcpyDeviceToHost, p->stream), "read");
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    double v;
+    memcpy(&v, &bits, sizeof(v));
+    *out = v;
+    GP5_CATCH
+}
+
+void gp5cu_functional_desc_init(gp5cu_functional_desc *d) {
+    if (!d) return;
+    memset(d, 0, sizeof(*d));
+    d->kind = GP5_FUNC_LHY;
+    d->c3 = -3.0;
+    d->c4 = 2.5;
+    d->masses[0] = d->masses[1] = 1.0;
+    d->potential = GP5_POT_NONE;
+}
+
+int gp5cu_functional_create(gp5cu_plan *p, const gp5cu_functional_desc *desc, gp5cu_functional **out) {
+    GP5_TRY
+    require(p && desc && out, "NULL argument");
+    *out = nullptr;
+    require(desc->kind >= GP5_FUNC_GP && desc->kind <= GP5_FUNC_LHY_UNLOCKED, "unknown functional kind");
+    require(desc->kind != GP5_FUNC_LHY_UNLOCKED || p->ncomp == 2, "the unlocked LHY functional needs 2 components");
+    require(desc->kind != GP5_FUNC_LHY || p->ncomp == 1, "the LHY droplet functional has 1 component");
+    require(desc->potential >= GP5_POT_NONE && desc->potential <= GP5_POT_ARRAY, "unknown potential kind");
+    require(desc->potential != GP5_POT_ARRAY || desc->dpotential != nullptr, "potential array is NULL");
+    use_device(p);
+    gp5cu_functional *f = new gp5cu_functional();
+    f->plan = p;
+    f->desc = *desc;
+    try {
+        for (int c = 0; c < p->ncomp; c++) {
+            const double m = (desc->kind == GP5_FUNC_GP) ? desc->masses[c] : 1.0;
+            require(m > 0, "masses must be positive");
+            // -1/2 (1/m) IFFT(-K^2 FFT)/N^3 = IFFT(K^2 FFT) * (0.5/m/N^3)
+            f->coef[c] = 0.5 * (1.0 / m) / (double)p->nsites;
+        }
+        if (desc->potential == GP5_POT_HARMONIC) {
+            // (w_d * w_d * x * x) per axis and component (externalPotential.cpp:26)
+            double **tabs[3] = {&f->hx, &f->hy, &f->hz};
+            for (int d = 0; d < 3; d++) {
+                const int n = p->shape[d];
+                std::vector<double> h((size_t)n * p->ncomp);
+                for (int c = 0; c < p->ncomp; c++)
+                    for (int i = 0; i < n; i++) {
+                        const double w = desc->omegas[c][d], x = p->pos_host[d][i];
+                        h[(size_t)c * n + i] = w * w * x * x;
+                    }
+                check_cuda(cudaMalloc(tabs[d], sizeof(double) * h.size()), "cudaMalloc harmonic");
+                check_cuda(cudaMemcpy(*tabs[d], h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice),
+                           "upload harmonic");
+            }
+        }
+    } catch (...) {
+        gp5cu_functional_destroy(f);
+        throw;
+    }
+    *out = f;
+    GP5_CATCH
+}
+
+int gp5cu_functional_destroy(gp5cu_functional *f) {
+    if (!f) return GP5_OK;
+    cudaSetDevice(f->plan->dev);
+    cudaStreamSynchronize(f->plan->stream);
+    cudaFree(f->hx);
+    cudaFree(f->hy);
+    cudaFree(f->hz);
+    delete f;
+    return GP5_OK;
+}
+
+int gp5cu_apply_H(gp5cu_functional *f, const void *src, void *dst) {
+    GP5_TRY
+    require(f != nullptr, "functional is NULL");
+    check_field_ptr(src, "src");
+    check_field_ptr(dst, "dst");
+    require(src != dst, "src and dst must differ");
+    gp5cu_plan *p = f->plan;
+    use_device(p);
+    dispatch(p, [&](auto r) { Launch<decltype(r)>::apply_h(f, src, dst, false); });
+    GP5_CATCH
+}
+
+int gp5cu_observables(gp5cu_functional *f, const void *field, gp5cu_observables_t *out) {
+    GP5_TRY
+    require(f && out, "NULL argument");
+    check_field_ptr(field, "field");
+    gp5cu_plan *p = f->plan;
+    use_device(p);
+    set_scalars(p->stream, p->ds);
+    dispatch(p, [&](auto r) {
+        // H psi lands in the workspace (read then written element by element by one thread)
+        Launch<decltype(r)>::apply_h(f, field, p->work, true);
+        Launch<decltype(r)>::residual(p, field, p->work, p->ds);
+    });
+    double s[8];
+    check_cuda(cudaMemcpyAsync(s, p->ds->sums, sizeof(s), cudaMemcpyDeviceToHost, p->stream), "read sums");
+    sync_and_check(p, p->ds);
+    const double dV = p->dV;
+    out->norm = s[0] * dV;
+    out->ekin = s[1] * dV;
+    out->epot = s[2] * dV;
+    out->eint = s[3] * dV;
+    out->energy = out->ekin + out->epot + out->eint;
+    out->mu = s[4] / s[0];
+    out->residual = sqrt(s[5] / s[0]);
+    GP5_CATCH
+}
+
+int gp5cu_stepper_create(gp5cu_functional *f, int kind, double dt, int imaginary, gp5cu_stepper **out) {
+    GP5_TRY
+    require(f && out, "NULL argument");
+    *out = nullptr;
+    require(kind == GP5_STEP_EULER || kind == GP5_STEP_RK4, "stepper kind must be GP5_STEP_EULER or GP5_STEP_RK4");
+    require(std::isfinite(dt), "time step must be finite");
+    gp5cu_plan *p = f->plan;
+    use_device(p);
+    gp5cu_stepper *st = new gp5cu_stepper();
+    st->func = f;
+    st->kind = kind;
+    st->dt = dt;
+    st->imaginary = imaginary ? 1 : 0;
+    // gpCpp.cpp:217-224: (dt, 0) imaginary, (0, dt) real
+    st->tre = imaginary ? dt : 0.0;
+    st->tim = imaginary ? 0.0 : dt;
+    try {
+        check_cuda(cudaMalloc(&st->Ka, p->field_bytes), "cudaMalloc k buffers");
+        if (kind == GP5_STEP_RK4) check_cuda(cudaMalloc(&st->Kb, p->field_bytes), "cudaMalloc k buffers");
+        check_cuda(cudaMalloc(&st->ds, sizeof(DevScalars)), "cudaMalloc scalars");
+        check_cuda(cudaMemset(st->ds, 0, sizeof(DevScalars)), "memset scalars");
+        set_scalars(p->stream, st->ds);
+    } catch (...) {
+        gp5cu_stepper_destroy(st);
+        throw;
+    }
+    *out = st;
+    GP5_CATCH
+}
+
+int gp5cu_stepper_destroy(gp5cu_stepper *st) {
+    if (!st) return GP5_OK;
+    cudaSetDevice(st->func->plan->dev);
+    cudaStreamSynchronize(st->func->plan->stream);
+    if (st->exec) cudaGraphExecDestroy(st->exec);
+    cudaFree(st->Ka);
+    cudaFree(st->Kb);
+    cudaFree(st->ds);
+    cudaFree(st->phase_exp);
+    cudaFree(st->dstate);
+    delete st;
+    return GP5_OK;
+}
+
+static void drop_graph(gp5cu_stepper *st) {
+    if (st->exec) cudaGraphExecDestroy(st->exec);
+    st->exec = nullptr;
+    st->graph_field = nullptr;
+}
+
+int gp5cu_stepper_set_renormalization(gp5cu_stepper *st, int n, const double *N) {
+    GP5_TRY
+    require(st != nullptr, "stepper is NULL");
+    const gp5cu_plan *p = st->func->plan;
+    if (n == 0) {
+        st->renorm = false;
+    } else {
+        require(N != nullptr, "N is NULL");
+        require(n == p->ncomp, "one normalisation per component is required");
+        for (int c = 0; c < n; c++) require(N[c] > 0, "normalisations must be positive");
+        st->renorm = true;
+        st->N[0] = N[0];
+        st->N[1] = n > 1 ? N[1] : 0.0;
+    }
+    drop_graph(st);
+    GP5_CATCH
+}
+
+int gp5cu_stepper_set_phase_constraint(gp5cu_stepper *st, const void *dphase) {
+    GP5_TRY
+    require(st != nullptr, "stepper is NULL");
+    gp5cu_plan *p = st->func->plan;
+    use_device(p);
+    drop_graph(st);
+    if (!dphase) {
+        check_cuda(cudaStreamSynchronize(p->stream), "sync");
+        cudaFree(st->phase_exp);
+        st->phase_exp = nullptr;
+    } else {
+        check_field_ptr(dphase, "dphase");
+        if (!st->phase_exp) check_cuda(cudaMalloc(&st->phase_exp, p->field_bytes), "cudaMalloc phase");
+        dispatch(p, [&](auto r) { Launch<decltype(r)>::phase_exp(p, dphase, st->phase_exp); });
+        check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    }
+    GP5_CATCH
+}
+
+static int queue_step(gp5cu_stepper *st, void *field) {
+    int n = 0;
+    dispatch(st->func->plan, [&](auto r) { n = Launch<decltype(r)>::step(st, field); });
+    return n;
+}
+
+int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
+    GP5_TRY
+    require(st != nullptr, "stepper is NULL");
+    check_field_ptr(field, "field");
+    require(nsteps >= 0, "nsteps must be >= 0");
+    gp5cu_plan *p = st->func->plan;
+    use_device(p);
+    if (nsteps == 0) return GP5_OK;
+    set_scalars(p->stream, st->ds);
+    int done = 0;
+    if (!st->exec || st->graph_field != field) {
+        drop_graph(st);
+        // one eager step (sets kernel attributes), then capture a step into a graph
+        st->launches_per_step = queue_step(st, field);
+        st->t += st->dt;
+        done = 1;
+        if (nsteps > 1) {
+            cudaGraph_t g = nullptr;
+            check_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            try {
+                queue_step(st, field);
+            } catch (...) {
+                cudaStreamEndCapture(p->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            check_cuda(cudaStreamEndCapture(p->stream, &g), "end capture");
+            cudaError_t e = cudaGraphInstantiate(&st->exec, g, 0);
+            cudaGraphDestroy(g);
+            check_cuda(e, "cudaGraphInstantiate");
+            st->graph_field = field;
+        }
+    }
+    for (int i = done; i < nsteps; i++) {
+        check_cuda(cudaGraphLaunch(st->exec, p->stream), "cudaGraphLaunch");
+        st->t += st->dt;
+    }
+    if (st->renorm) {
+        // materialise the pending normalisation of the last step (stepper.cpp:67)
+        dispatch(p, [&](auto r) { Launch<decltype(r)>::scale(p, field, -1, st->ds, true); });
+    }
+    sync_and_check(p, st->ds);
+    GP5_CATCH
+}
+
+int gp5cu_stepper_get_time(const gp5cu_stepper *st, double *t) {
+    if (!st || !t) {
+        set_last_error("NULL argument");
+        return GP5_ERR_ARG;
+    }
+    *t = st->t;
+    return GP5_OK;
+}
+
+int gp5cu_stepper_set_time(gp5cu_stepper *st, double t) {
+    if (!st) {
+        set_last_error("stepper is NULL");
+        return GP5_ERR_ARG;
+    }
+    st->t = t;
+    return GP5_OK;
+}
+
+int gp5cu_stepper_advance_host(gp5cu_stepper *st, const void *host_in, void *host_out, int nsteps) {
+    GP5_TRY
+    require(st && host_in && host_out, "NULL argument");
+    require(nsteps >= 0, "nsteps must be >= 0");
+    gp5cu_plan *p = st->func->plan;
+    use_device(p);
+    if (!st->dstate) check_cuda(cudaMalloc(&st->dstate, p->field_bytes), "cudaMalloc state");
+    check_cuda(cudaMemcpyAsync(st->dstate, host_in, p->field_bytes, cudaMemcpyHostToDevice, p->stream), "upload");
+    const int rc = gp5cu_stepper_advance(st, st->dstate, nsteps);
+    if (rc != GP5_OK) return rc;
+    check_cuda(cudaMemcpyAsync(host_out, st->dstate, p->field_bytes, cudaMemcpyDeviceToHost, p->stream), "download");
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    GP5_CATCH
+}
+
+int gp5cu_stepper_launches_per_step(const gp5cu_stepper *st) { return st ? st->launches_per_step : 0; }
+
+int gp5cu_stepper_profile(gp5cu_stepper *st, void *field, int nrep, double *ms, int *kinds, int cap,
+                          int *nlaunch) {
+    GP5_TRY
+    require(st && ms && kinds && nlaunch, "NULL argument");
+    check_field_ptr(field, "field");
+    require(nrep >= 1, "nrep must be >= 1");
+    gp5cu_plan *p = st->func->plan;
+    use_device(p);
+    ProfRec rec;
+    p->prof = &rec;
+    try {
+        set_scalars(p->stream, st->ds);
+        std::vector<double> acc;
+        int n = 0;
+        for (int r = 0; r < nrep; r++) {
+            rec.idx = 0;
+            rec.record(p->stream, -1);
+            n = queue_step(st, field);
+            st->t += st->dt;
+            check_cuda(cudaStreamSynchronize(p->stream), "sync");
+            if (acc.empty()) acc.assign(rec.idx - 1, 0.0);
+            for (size_t i = 1; i < rec.idx; i++) {
+                float t = 0;
+                check_cuda(cudaEventElapsedTime(&t, rec.ev[i - 1], rec.ev[i]), "cudaEventElapsedTime");
+                acc[i - 1] += t;
+            }
+        }
+        (void)n;
+        const int m = (int)acc.size();
+        *nlaunch = m;
+        for (int i = 0; i < m && i < cap; i++) {
+            ms[i] = acc[i] / nrep;
+            kinds[i] = rec.kinds[i + 1];
+        }
+        if (st->renorm) dispatch(p, [&](auto r) { Launch<decltype(r)>::scale(p, field, -1, st->ds, true); });
+        sync_and_check(p, st->ds);
+    } catch (...) {
+        p->prof = nullptr;
+        for (auto e : rec.ev) cudaEventDestroy(e);
+        throw;
+    }
+    p->prof = nullptr;
+    for (auto e : rec.ev) cudaEventDestroy(e);
+    GP5_CATCH
+}
+
+}  // extern "C"

@@ -1,0 +1,370 @@
+// launch_impl.cuh - precision-templated launchers: tile geometry, engine dispatch and the
+// kernel sequences of the transforms, the H application and one stepper step.
+// Included once per precision (gp5cu_f64.cu, gp5cu_f32.cu).
+#pragma once
+
+#include <algorithm>
+#include <cstdio>
+
+#include "ops.cuh"
+#include "plan.hpp"
+
+namespace gp5 {
+
+constexpr int kThreads = 256;
+
+inline TileGeom make_geom(const gp5cu_plan *p, int axis, int lines, bool pow2_bx, long long *tiles) {
+    TileGeom g{};
+    g.nx = p->shape[0];
+    g.ny = p->shape[1];
+    g.nz = p->shape[2];
+    g.nc = p->ncomp;
+    g.axis = axis;
+    g.n = p->shape[axis];
+    g.estride = axis == 0 ? 1 : (axis == 1 ? (long long)g.nx : (long long)g.nx * g.ny);
+    if (axis == 0) {
+        g.lines = lines;
+        g.bx = g.bo = 1;
+        g.tiles_x = 1;
+        g.n_other = (long long)g.ny * g.nz * g.nc;
+        *tiles = (g.n_other + lines - 1) / lines;
+    } else {
+        int bx = std::min(lines, g.nx);
+        if (pow2_bx) {
+            int b = 1;
+            while (b * 2 <= bx) b *= 2;
+            bx = b;
+        }
+        const int bo = lines / bx;
+        g.lines = bx * bo;
+        g.bx = bx;
+        g.bo = bo;
+        g.tiles_x = (g.nx + bx - 1) / bx;
+        g.n_other = axis == 1 ? (long long)g.nz * g.nc : (long long)g.ny * g.nc;
+        *tiles = (long long)g.tiles_x * ((g.n_other + bo - 1) / bo);
+    }
+    return g;
+}
+
+inline RedSlot red_slot(const gp5cu_plan *p) { return RedSlot{p->partials, p->counter}; }
+
+template <class K> inline void ensure_smem(K kernel, size_t bytes, int dev) {
+    static bool done[64] = {false};
+    if (bytes > 48 * 1024 && dev < 64 && !done[dev]) {
+        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                   "cudaFuncSetAttribute");
+        done[dev] = true;
+    }
+}
+
+template <typename Real, int N, bool CONTIG, int MODE, class Op>
+void launch_reg(gp5cu_plan *p, int axis, const Op &op) {
+    using V = cpx<Real>;
+    constexpr int LINES = RegTile<N>::LINES;
+    long long tiles = 0;
+    TileGeom g = make_geom(p, axis, LINES, true, &tiles);
+    const size_t smem = CONTIG ? (size_t)LINES * LayContig<N>::LD * sizeof(V) : (size_t)LINES * N * sizeof(V);
+    auto kern = k_axis_reg<Real, N, CONTIG, MODE, Op>;
+    ensure_smem(kern, smem, p->dev);
+    kern<<<(unsigned)tiles, kThreads, smem, p->stream>>>(g, op, (const V *)p->ax[axis].tw, red_slot(p));
+    check_cuda(cudaGetLastError(), "k_axis_reg launch");
+    if (p->prof) p->prof->record(p->stream, axis * 10 + MODE);
+}
+
+template <typename Real, bool CONTIG, int MODE, class Op>
+void launch_smem(gp5cu_plan *p, int axis, const Op &op) {
+    using V = cpx<Real>;
+    const AxisPlan &ap = p->ax[axis];
+    long long tiles = 0;
+    TileGeom g = make_geom(p, axis, ap.smem_lines, false, &tiles);
+    const int ld = CONTIG ? g.n + 1 : g.lines;
+    const size_t bufsz = CONTIG ? (size_t)g.lines * ld : (size_t)g.lines * g.n;
+    const size_t smem = 2 * bufsz * sizeof(V);
+    auto kern = k_axis_smem<Real, CONTIG, MODE, Op>;
+    ensure_smem(kern, smem, p->dev);
+    kern<<<(unsigned)tiles, kThreads, smem, p->stream>>>(g, ap.sched, op, (const V *)ap.tw, red_slot(p));
+    check_cuda(cudaGetLastError(), "k_axis_smem launch");
+    if (p->prof) p->prof->record(p->stream, axis * 10 + MODE);
+}
+
+template <typename Real, bool CONTIG, int MODE, class Op>
+void launch_axis(gp5cu_plan *p, int axis, const Op &op) {
+    const AxisPlan &ap = p->ax[axis];
+    if (ap.reg) {
+        switch (ap.n) {
+            case 32: launch_reg<Real, 32, CONTIG, MODE>(p, axis, op); return;
+            case 64: launch_reg<Real, 64, CONTIG, MODE>(p, axis, op); return;
+            case 128: launch_reg<Real, 128, CONTIG, MODE>(p, axis, op); return;
+            case 256: launch_reg<Real, 256, CONTIG, MODE>(p, axis, op); return;
+            case 512: launch_reg<Real, 512, CONTIG, MODE>(p, axis, op); return;
+            default: break;
+        }
+    }
+    launch_smem<Real, CONTIG, MODE>(p, axis, op);
+}
+
+template <class Op> void launch_pointwise(gp5cu_plan *p, const Op &op) {
+    k_pointwise<Op><<<p->pw_blocks, kThreads, 0, p->stream>>>(p->nsites, op, red_slot(p));
+    check_cuda(cudaGetLastError(), "k_pointwise launch");
+    if (p->prof) p->prof->record(p->stream, 90);
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(256) k_max_density(const cpx<Real> *f, long long nsites, int ncomp,
+                                                     unsigned long long *out) {
+    double m = 0.0;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsites;
+         s += (long long)gridDim.x * blockDim.x) {
+        for (int c = 0; c < ncomp; c++) {
+            const cpx<Real> v = f[s + (long long)c * nsites];
+            const double n = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+            m = fmax(m, n);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    __shared__ double wm[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) wm[w] = m;
+    __syncthreads();
+    if (w == 0) {
+        m = lane < (int)(blockDim.x >> 5) ? wm[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+        if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(256) k_phase_exp(const Real *phase, cpx<Real> *out, long long n) {
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (long long)gridDim.x * blockDim.x) {
+        Real sn, cs;
+        sincos(phase[s], &sn, &cs);
+        out[s] = mk<Real>(cs, sn);
+    }
+}
+
+// ---- transforms ----------------------------------------------------------------------------
+template <typename Real> void Launch<Real>::fft(gp5cu_plan *p, const void *src, void *dst, int dir) {
+    using V = cpx<Real>;
+    const V *s = (const V *)src;
+    V *d = (V *)dst;
+    if (dir == GP5_FORWARD) {
+        OpStageIn<Real, false> in{};
+        in.psi = s;
+        in.kprev = nullptr;
+        in.dst = d;
+        launch_axis<Real, true, MODE_FWD>(p, 0, in);
+        OpCopy<Real> cp{d, d};
+        launch_axis<Real, false, MODE_FWD>(p, 1, cp);
+        launch_axis<Real, false, MODE_FWD>(p, 2, cp);
+    } else {
+        OpCopy<Real> first{s, d};
+        launch_axis<Real, true, MODE_INV>(p, 0, first);
+        OpCopy<Real> cp{d, d};
+        launch_axis<Real, false, MODE_INV>(p, 1, cp);
+        launch_axis<Real, false, MODE_INV>(p, 2, cp);
+    }
+}
+
+template <typename Real>
+static void kinetic_passes(gp5cu_plan *p, const void *src, void *w, double coef0, double coef1) {
+    using V = cpx<Real>;
+    OpStageIn<Real, false> in{};
+    in.psi = (const V *)src;
+    in.kprev = nullptr;
+    in.dst = (V *)w;
+    launch_axis<Real, true, MODE_FWD>(p, 0, in);
+    OpCopy<Real> cp{(const V *)w, (V *)w};
+    launch_axis<Real, false, MODE_FWD>(p, 1, cp);
+    OpKinetic<Real> kin{(const V *)w, (V *)w, p->k2[0], p->k2[1], p->k2[2], coef0, coef1};
+    launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
+    launch_axis<Real, false, MODE_INV>(p, 1, cp);
+}
+
+template <typename Real> void Launch<Real>::laplacian(gp5cu_plan *p, const void *src, void *dst) {
+    using V = cpx<Real>;
+    const double c = -1.0 / (double)p->nsites;
+    kinetic_passes<Real>(p, src, p->work, c, c);
+    OpCopy<Real> last{(const V *)p->work, (V *)dst};
+    launch_axis<Real, true, MODE_INV>(p, 0, last);
+}
+
+template <typename Real> static EpiParams<Real> base_epi(gp5cu_functional *f) {
+    const gp5cu_plan *p = f->plan;
+    const gp5cu_functional_desc &d = f->desc;
+    EpiParams<Real> P{};
+    P.nsites = p->nsites;
+    P.fkind = d.kind;
+    P.has_g = d.has_couplings;
+    P.g00 = (Real)d.couplings[0];
+    P.g01 = (Real)d.couplings[1];
+    P.g11 = (Real)d.couplings[3];
+    P.c3 = (Real)d.c3;
+    P.c4 = (Real)d.c4;
+    P.la = (Real)d.alpha;
+    P.lb = (Real)d.beta;
+    P.le = (Real)d.eta;
+    P.pot = d.potential;
+    P.hx = f->hx;
+    P.hy = f->hy;
+    P.hz = f->hz;
+    P.nx = p->shape[0];
+    P.ny = p->shape[1];
+    P.nz = p->shape[2];
+    P.varr = (const Real *)d.dpotential;
+    P.dV = p->dV;
+    return P;
+}
+
+template <typename Real>
+static void epilogue(gp5cu_plan *p, const EpiParams<Real> &P, bool red) {
+    using V = cpx<Real>;
+    if (p->ncomp == 1) {
+        if (red) {
+            OpStageOut<Real, true> op{(const V *)p->work, P};
+            launch_axis<Real, true, MODE_INV>(p, 0, op);
+        } else {
+            OpStageOut<Real, false> op{(const V *)p->work, P};
+            launch_axis<Real, true, MODE_INV>(p, 0, op);
+        }
+    } else {
+        OpCopy<Real> cp{(const V *)p->work, (V *)p->work};
+        launch_axis<Real, true, MODE_INV>(p, 0, cp);
+        EpiParams<Real> Q = P;
+        Q.tsrc = (const V *)p->work;
+        if (red) launch_pointwise(p, OpSiteEpilogue<Real, 2, true>{Q});
+        else launch_pointwise(p, OpSiteEpilogue<Real, 2, false>{Q});
+    }
+}
+
+template <typename Real>
+void Launch<Real>::apply_h(gp5cu_functional *f, const void *src, void *dst, bool obs) {
+    using V = cpx<Real>;
+    gp5cu_plan *p = f->plan;
+    kinetic_passes<Real>(p, src, p->work, f->coef[0], f->coef[1]);
+    EpiParams<Real> P = base_epi<Real>(f);
+    P.mode = obs ? EPI_OBS : EPI_H;
+    P.psi = (const V *)src;
+    P.kout = (V *)dst;
+    P.ds = p->ds;
+    epilogue<Real>(p, P, obs);
+}
+
+template <typename Real>
+void Launch<Real>::residual(gp5cu_plan *p, const void *psi, const void *hpsi, DevScalars *ds) {
+    using V = cpx<Real>;
+    OpResidual<Real> op{(const V *)psi, (const V *)hpsi, p->nsites, p->ncomp, ds};
+    launch_pointwise(p, op);
+}
+
+template <typename Real>
+void Launch<Real>::norm(gp5cu_plan *p, const void *field, int comp, double Ntarget, DevScalars *ds) {
+    using V = cpx<Real>;
+    OpNorm<Real> op{(const V *)field, p->nsites, comp, p->ncomp, ds, Ntarget, p->dV};
+    launch_pointwise(p, op);
+}
+
+template <typename Real>
+void Launch<Real>::scale(gp5cu_plan *p, void *field, int comp, DevScalars *ds, bool from_sigma) {
+    using V = cpx<Real>;
+    OpScale<Real> op{(V *)field, p->nsites, comp, p->ncomp, ds, from_sigma ? 1 : 0};
+    launch_pointwise(p, op);
+}
+
+template <typename Real> void Launch<Real>::max_density(gp5cu_plan *p, const void *field) {
+    check_cuda(cudaMemsetAsync(p->dmax, 0, sizeof(unsigned long long), p->stream), "memset");
+    k_max_density<Real><<<p->pw_blocks, kThreads, 0, p->stream>>>((const cpx<Real> *)field, p->nsites,
+                                                                    p->ncomp, p->dmax);
+    check_cuda(cudaGetLastError(), "k_max_density launch");
+}
+
+template <typename Real>
+void Launch<Real>::convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128) {
+    OpConvert<Real> op{(const double2 *)in128, (cpx<Real> *)out, (const cpx<Real> *)in, (double2 *)out128};
+    k_pointwise<OpConvert<Real>><<<p->pw_blocks, kThreads, 0, p->stream>>>(p->nsites * p->ncomp, op,
+                                                                           red_slot(p));
+    check_cuda(cudaGetLastError(), "convert launch");
+}
+
+template <typename Real> void Launch<Real>::phase_exp(gp5cu_plan *p, const void *phase, void *out) {
+    k_phase_exp<Real><<<p->pw_blocks, kThreads, 0, p->stream>>>((const Real *)phase, (cpx<Real> *)out,
+                                                                 p->nsites * p->ncomp);
+    check_cuda(cudaGetLastError(), "phase_exp launch");
+}
+
+// ---- one stepper step ----------------------------------------------------------------------
+// RK4 (stepper.cpp:46-71) as four stages of five axis passes each:
+//   x fwd [u~ = sigma psi0 - c k_{s-1}, |u~|^2]  y fwd  z fwd*K^2/(2mN^3)*z inv  y inv
+//   x inv [k_s = H(alpha u~); RK bookkeeping; psi1 on the last stage]
+// Buffers: psi (in/out, in place), work (transform), Ka (k1, then the running sum
+// k1 + 2k2 + 2k3), Kb (k2, then k3).
+template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) {
+    using V = cpx<Real>;
+    gp5cu_functional *f = st->func;
+    gp5cu_plan *p = f->plan;
+    V *psi = (V *)field;
+    V *W = (V *)p->work;
+    V *Ka = (V *)st->Ka;
+    V *Kb = (V *)st->Kb;
+    const bool rk4 = st->kind == GP5_STEP_RK4;
+    const int nst = rk4 ? 4 : 1;
+    int launches = 0;
+    for (int s = 1; s <= nst; s++) {
+        double cre = 0, cim = 0;
+        const V *kprev = nullptr;
+        if (rk4 && s > 1) {
+            const double a = (s == 4) ? 1.0 : 0.5;
+            cre = st->tre * a;
+            cim = st->tim * a;
+            kprev = (s == 2) ? Ka : Kb;
+        }
+        const bool red_in = st->renorm && rk4 && s > 1;
+        if (red_in) {
+            OpStageIn<Real, true> in{psi, kprev, W, st->ds, 1, (Real)cre, (Real)cim, st->N[0], st->N[1], p->dV};
+            launch_axis<Real, true, MODE_FWD>(p, 0, in);
+        } else {
+            OpStageIn<Real, false> in{psi, kprev, W, st->ds, st->renorm ? 1 : 0, (Real)cre, (Real)cim, 0, 0, p->dV};
+            launch_axis<Real, true, MODE_FWD>(p, 0, in);
+        }
+        OpCopy<Real> cp{W, W};
+        launch_axis<Real, false, MODE_FWD>(p, 1, cp);
+        OpKinetic<Real> kin{W, W, p->k2[0], p->k2[1], p->k2[2], f->coef[0], f->coef[1]};
+        launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
+        launch_axis<Real, false, MODE_INV>(p, 1, cp);
+        launches += 4;
+
+        EpiParams<Real> P = base_epi<Real>(f);
+        P.ds = st->ds;
+        P.psi = psi;
+        P.psi_out = psi;
+        P.kprev = kprev;
+        P.kacc = Ka;
+        P.use_sigma = st->renorm ? 1 : 0;
+        P.use_alpha = red_in ? 1 : 0;
+        P.cre = (Real)cre;
+        P.cim = (Real)cim;
+        P.phase_exp = nullptr;
+        if (!rk4) {
+            P.mode = EPI_EULER;
+            P.dre = (Real)st->tre;
+            P.dim = (Real)st->tim;
+        } else {
+            P.mode = EPI_RK1 + (s - 1);
+            P.kout = (s == 1) ? Ka : Kb;
+            P.dre = (Real)(st->tre * (1. / 6));
+            P.dim = (Real)(st->tim * (1. / 6));
+        }
+        const bool last = (s == nst);
+        if (last) {
+            P.phase_exp = (const V *)st->phase_exp;
+            P.renorm_out = st->renorm ? 1 : 0;
+            P.Nt0 = st->N[0];
+            P.Nt1 = st->N[1];
+        }
+        epilogue<Real>(p, P, last && st->renorm);
+        launches += (p->ncomp == 1) ? 1 : 2;
+    }
+    return launches;
+}
+
+}  // namespace gp5

@@ -1,0 +1,331 @@
+// passes.cuh - axis-pass kernels: one kernel = a batch of line FFTs along one axis, with
+// the point-wise work of the stepper fused into its loads (prologue), into the middle of a
+// forward+inverse pair (kinetic multiply), and into its stores (epilogue).
+//
+// Field layout: element (i, j, k, c) at i + nx*(j + ny*(k + nz*c)) (ColMajor, x fastest).
+//   x axis: a line is contiguous; a tile is LINES consecutive lines.
+//   y/z axes: a line has stride nx (y) or nx*ny (z); a tile is bx consecutive x values by bo
+//     other lines, so that a warp's loads cover bx*16 contiguous bytes per position.
+//
+// Reductions: every op may accumulate up to 8 FP64 sums per thread.  A block folds them
+// with a fixed-order shuffle tree, writes one partial per block, and the last block to
+// finish (atomic ticket, no waiting) adds the partials in index order with Neumaier
+// compensation and calls op.finalize.  The result is independent of block scheduling, so
+// repeated runs are bitwise identical.
+#pragma once
+
+#include "common.cuh"
+#include "fft_line.cuh"
+
+namespace gp5 {
+
+enum PassMode : int { MODE_FWD = 0, MODE_INV = 1, MODE_FWD_MID_INV = 2 };
+
+struct TileGeom {
+    int nx, ny, nz, nc;
+    int axis;           // 0 = x, 1 = y, 2 = z
+    int n;              // line length
+    long long estride;  // element stride along the line
+    int lines;          // lines per tile
+    int bx, bo;         // strided tiles: consecutive x lines, other lines
+    int tiles_x;        // strided tiles: ceil(nx / bx)
+    long long n_other;  // strided: number of (other) line groups; x axis: total lines
+};
+
+struct RedSlot {
+    double *partials;   // [gridDim.x * 8]
+    unsigned *counter;  // zero between launches
+};
+
+// Coordinates of one line: base offset and the fixed coordinates.
+struct LineRef {
+    long long base;
+    int i, j, k, c;
+    bool valid;
+};
+
+__device__ __forceinline__ LineRef line_ref(const TileGeom &g, long long tile, int line) {
+    LineRef r;
+    r.i = r.j = r.k = r.c = 0;
+    if (g.axis == 0) {
+        long long L = tile * g.lines + line;
+        r.valid = L < g.n_other;
+        if (!r.valid) L = 0;
+        r.base = L * g.nx;
+        r.j = (int)(L % g.ny);
+        long long t = L / g.ny;
+        r.k = (int)(t % g.nz);
+        r.c = (int)(t / g.nz);
+    } else {
+        const long long tx = tile % g.tiles_x, to = tile / g.tiles_x;
+        const int xo = line % g.bx, oo = line / g.bx;
+        int i = (int)(tx * g.bx) + xo;
+        long long o = to * g.bo + oo;
+        r.valid = (i < g.nx) && (o < g.n_other);
+        if (!r.valid) { i = 0; o = 0; }
+        r.i = i;
+        if (g.axis == 1) {  // o = k + nz*c
+            r.k = (int)(o % g.nz);
+            r.c = (int)(o / g.nz);
+            r.base = i + (long long)g.nx * g.ny * o;
+        } else {            // o = j + ny*c
+            r.j = (int)(o % g.ny);
+            r.c = (int)(o / g.ny);
+            r.base = i + (long long)g.nx * r.j + (long long)g.nx * g.ny * g.nz * r.c;
+        }
+    }
+    return r;
+}
+
+__device__ __forceinline__ void set_pos(const TileGeom &g, LineRef &r, int pos) {
+    if (g.axis == 0) r.i = pos;
+    else if (g.axis == 1) r.j = pos;
+    else r.k = pos;
+}
+
+// ---- reductions -------------------------------------------------------------------------
+template <int K> __device__ __forceinline__ void warp_sum(double (&a)[K]) {
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) a[r] += __shfl_down_sync(0xffffffffu, a[r], off);
+    }
+}
+
+// Block sum in fixed order; result valid in thread 0.
+template <int K> __device__ void block_sum(double (&a)[K]) {
+    __shared__ double red[32 * (K > 0 ? K : 1)];
+    warp_sum<K>(a);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < K; r++) red[w * K + r] = a[r];
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int r = 0; r < K; r++) a[r] = lane < nw ? red[lane * K + r] : 0.0;
+        warp_sum<K>(a);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void neumaier(double &s, double &comp, double x) {
+    double t = s + x;
+    if (fabs(s) >= fabs(x)) comp += (s - t) + x;
+    else comp += (x - t) + s;
+    s = t;
+}
+
+// Per-block partials, then the last block folds them and calls op.finalize(sums).
+template <int K, class Op>
+__device__ void reduce_and_finalize(const double *acc_in, const RedSlot &rs, const Op &op) {
+    if constexpr (K > 0) {
+        double acc[K];
+#pragma unroll
+        for (int r = 0; r < K; r++) acc[r] = acc_in[r];
+        block_sum<K>(acc);
+        const long long nblocks = (long long)gridDim.x;
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int r = 0; r < K; r++) rs.partials[(long long)blockIdx.x * K + r] = acc[r];
+        }
+        __threadfence();
+        __shared__ bool s_last;
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = (atomicAdd(rs.counter, 1u) == (unsigned)(nblocks - 1));
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            double s[K], cp[K];
+#pragma unroll
+            for (int r = 0; r < K; r++) { s[r] = 0.0; cp[r] = 0.0; }
+            for (long long b = threadIdx.x; b < nblocks; b += blockDim.x) {
+#pragma unroll
+                for (int r = 0; r < K; r++) neumaier(s[r], cp[r], __ldcg(rs.partials + b * K + r));
+            }
+            block_sum<K>(s);
+            block_sum<K>(cp);
+            if (threadIdx.x == 0) {
+                double tot[K];
+#pragma unroll
+                for (int r = 0; r < K; r++) tot[r] = s[r] + cp[r];
+                op.finalize(tot);
+                *rs.counter = 0u;
+            }
+        }
+    }
+}
+
+// ---- register-engine kernel ----------------------------------------------------------------
+// Threads: LINES lines x T threads per line; 256 threads for every supported N.
+template <int N> struct RegTile {
+    static constexpr int T = RegCfgAll<N>::T;
+    static constexpr int LINES = 256 / T;
+};
+
+template <typename Real, int N, bool CONTIG, int MODE, class Op>
+__global__ void __launch_bounds__(256, 2)
+k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedSlot rs) {
+    using V = cpx<Real>;
+    constexpr int E = RegCfg<N>::E, T = RegCfgAll<N>::T, LINES = RegTile<N>::LINES;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *sm = reinterpret_cast<V *>(smem_raw);
+
+    int tid, line;
+    if (CONTIG) { tid = threadIdx.x % T; line = threadIdx.x / T; }
+    else { line = threadIdx.x % LINES; tid = threadIdx.x / LINES; }
+
+    LineRef lr = line_ref(g, blockIdx.x, line);
+    double acc[Op::NRED > 0 ? Op::NRED : 1];
+#pragma unroll
+    for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); r++) acc[r] = 0.0;
+
+    V v[E];
+#pragma unroll
+    for (int m = 0; m < E; m++) {
+        const int pos = tid + T * m;
+        if (lr.valid) {
+            LineRef e = lr;
+            set_pos(g, e, pos);
+            v[m] = op.load(lr.base + pos * g.estride, e, acc);
+        } else {
+            v[m] = mk<Real>(0, 0);
+        }
+    }
+    if constexpr (CONTIG) {
+        LayContig<N> lay;
+        if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+        else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+        if (MODE == MODE_FWD_MID_INV) {
+#pragma unroll
+            for (int m = 0; m < E; m++) {
+                LineRef e = lr;
+                set_pos(g, e, tid + T * m);
+                v[m] = op.mid(v[m], e);
+            }
+            __syncthreads();
+            reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+        }
+    } else {
+        LayStrided lay{LINES};
+        if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+        else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+        if (MODE == MODE_FWD_MID_INV) {
+#pragma unroll
+            for (int m = 0; m < E; m++) {
+                LineRef e = lr;
+                set_pos(g, e, tid + T * m);
+                v[m] = op.mid(v[m], e);
+            }
+            __syncthreads();
+            reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+        }
+    }
+    if (lr.valid) {
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            const int pos = tid + T * m;
+            LineRef e = lr;
+            set_pos(g, e, pos);
+            op.store(lr.base + pos * g.estride, e, v[m], acc);
+        }
+    }
+    reduce_and_finalize<Op::NRED>(acc, rs, op);
+}
+
+// ---- shared-memory-engine kernel (any length) ---------------------------------------------
+struct LayContigRT {
+    int ld;
+    __device__ __forceinline__ int operator()(int line, int pos) const { return line * ld + pos; }
+};
+
+template <typename Real, bool CONTIG, int MODE, class Op>
+__global__ void __launch_bounds__(256)
+k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__restrict__ tw,
+            const RedSlot rs) {
+    using V = cpx<Real>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = g.n, lines = g.lines;
+    const int ld = CONTIG ? n + 1 : lines;
+    const int bufsz = CONTIG ? lines * ld : lines * n;
+    V *b0 = reinterpret_cast<V *>(smem_raw);
+    V *b1 = b0 + bufsz;
+    constexpr int K = Op::NRED > 0 ? Op::NRED : 1;
+    double acc[K];
+#pragma unroll
+    for (int r = 0; r < K; r++) acc[r] = 0.0;
+
+    auto lay_idx = [&](int line, int pos) { return CONTIG ? line * ld + pos : pos * lines + line; };
+    const int total = lines * n;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        int line, pos;
+        if (CONTIG) { pos = q % n; line = q / n; }
+        else { line = q % lines; pos = q / lines; }
+        LineRef lr = line_ref(g, blockIdx.x, line);
+        V val = mk<Real>(0, 0);
+        if (lr.valid) {
+            set_pos(g, lr, pos);
+            val = op.load(lr.base + pos * g.estride, lr, acc);
+        }
+        b0[lay_idx(line, pos)] = val;
+    }
+    __syncthreads();
+    V *res;
+    if (CONTIG) {
+        LayContigRT lay{ld};
+        res = (MODE == MODE_INV) ? smem_fft<1>(b0, b1, lines, ls, tw, lay)
+                                 : smem_fft<-1>(b0, b1, lines, ls, tw, lay);
+    } else {
+        LayStrided lay{lines};
+        res = (MODE == MODE_INV) ? smem_fft<1>(b0, b1, lines, ls, tw, lay)
+                                 : smem_fft<-1>(b0, b1, lines, ls, tw, lay);
+    }
+    if (MODE == MODE_FWD_MID_INV) {
+        for (int q = threadIdx.x; q < total; q += blockDim.x) {
+            int line, pos;
+            if (CONTIG) { pos = q % n; line = q / n; }
+            else { line = q % lines; pos = q / lines; }
+            LineRef lr = line_ref(g, blockIdx.x, line);
+            set_pos(g, lr, pos);
+            const int s = lay_idx(line, pos);
+            res[s] = op.mid(res[s], lr);
+        }
+        __syncthreads();
+        V *other = (res == b0) ? b1 : b0;
+        if (CONTIG) {
+            LayContigRT lay{ld};
+            res = smem_fft<1>(res, other, lines, ls, tw, lay);
+        } else {
+            LayStrided lay{lines};
+            res = smem_fft<1>(res, other, lines, ls, tw, lay);
+        }
+    }
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        int line, pos;
+        if (CONTIG) { pos = q % n; line = q / n; }
+        else { line = q % lines; pos = q / lines; }
+        LineRef lr = line_ref(g, blockIdx.x, line);
+        if (lr.valid) {
+            set_pos(g, lr, pos);
+            op.store(lr.base + pos * g.estride, lr, res[lay_idx(line, pos)], acc);
+        }
+    }
+    reduce_and_finalize<Op::NRED>(acc, rs, op);
+}
+
+// ---- point-wise kernel over all sites (reductions, scaling, conversions) -----------------
+template <class Op>
+__global__ void __launch_bounds__(256) k_pointwise(const long long nsites, Op op, const RedSlot rs) {
+    constexpr int K = Op::NRED > 0 ? Op::NRED : 1;
+    double acc[K];
+#pragma unroll
+    for (int r = 0; r < K; r++) acc[r] = 0.0;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsites;
+         s += (long long)gridDim.x * blockDim.x)
+        op.site(s, acc);
+    reduce_and_finalize<Op::NRED>(acc, rs, op);
+}
+
+}  // namespace gp5

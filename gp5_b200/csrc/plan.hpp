@@ -1,0 +1,115 @@
+// plan.hpp - host-side objects behind the C ABI (opaque to callers).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gp5cu.h"
+#include "ops.cuh"
+
+namespace gp5 {
+
+// Optional per-launch timing: when a plan has a recorder, every kernel launch is followed by
+// an event on the plan stream, and kinds[i] labels launch i (axis*10 + mode, or 90 for a
+// point-wise kernel).
+struct ProfRec {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kinds;
+    size_t idx = 0;
+    void record(cudaStream_t s, int kind);
+};
+
+struct AxisPlan {
+    int n = 0;
+    bool reg = false;     // register engine (power of two in [32, 512])
+    LineSchedule sched{};  // mixed-radix schedule for the shared-memory engine
+    void *tw = nullptr;    // device twiddle table, plan precision, forward sign
+    int smem_lines = 0;    // lines per tile of the shared-memory engine
+};
+
+// Thrown inside the library, caught at the C boundary and turned into a status code.
+struct Gp5Error {
+    int status;
+    std::string msg;
+};
+
+void set_last_error(const std::string &msg);
+[[noreturn]] void fail(int status, const std::string &msg);
+void check_cuda(cudaError_t e, const char *what);
+
+}  // namespace gp5
+
+struct gp5cu_plan {
+    int dev = 0;
+    int shape[3] = {0, 0, 0};
+    double left[3] = {0, 0, 0}, right[3] = {0, 0, 0};
+    int ncomp = 1;
+    int prec = GP5_C128;
+    long long nsites = 0;  // nx*ny*nz
+    size_t elem_bytes = 16;
+    size_t field_bytes = 0;
+    double dV = 1.0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    gp5::AxisPlan ax[3];
+    double *k2[3] = {nullptr, nullptr, nullptr};  // device k_d^2
+    std::vector<double> pos_host[3];              // cell-centred coordinates
+    void *work = nullptr;                         // one field of FFT workspace
+    double *partials = nullptr;
+    unsigned *counter = nullptr;
+    long long max_blocks = 0;
+    gp5::DevScalars *ds = nullptr;
+    unsigned long long *dmax = nullptr;
+    int pw_blocks = 0;  // grid of the point-wise kernels
+    gp5::ProfRec *prof = nullptr;
+};
+
+struct gp5cu_functional {
+    gp5cu_plan *plan = nullptr;
+    gp5cu_functional_desc desc{};
+    double *hx = nullptr, *hy = nullptr, *hz = nullptr;  // harmonic tables [ncomp][n_d]
+    double coef[2] = {0, 0};                            // kinetic multiplier per component
+};
+
+struct gp5cu_stepper {
+    gp5cu_functional *func = nullptr;
+    int kind = GP5_STEP_RK4;
+    double dt = 0;
+    int imaginary = 1;
+    double tre = 0, tim = 0;  // complex time step
+    bool renorm = false;
+    double N[2] = {0, 0};
+    void *phase_exp = nullptr;  // e^{i phi}, plan precision, owned
+    void *Ka = nullptr, *Kb = nullptr;
+    void *dstate = nullptr;  // resident state of the host-buffer entry point
+    gp5::DevScalars *ds = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void *graph_field = nullptr;
+    bool graph_renorm = false;
+    const void *graph_phase = nullptr;
+    double t = 0;
+    int launches_per_step = 0;
+};
+
+namespace gp5 {
+
+// precision-specific launchers (gp5cu_kernels_f64.cu / gp5cu_kernels_f32.cu)
+template <typename Real> struct Launch {
+    static void fft(gp5cu_plan *p, const void *src, void *dst, int dir);
+    static void laplacian(gp5cu_plan *p, const void *src, void *dst);
+    static void apply_h(gp5cu_functional *f, const void *src, void *dst, bool obs);
+    static void residual(gp5cu_plan *p, const void *psi, const void *hpsi, DevScalars *ds);
+    static void norm(gp5cu_plan *p, const void *field, int comp, double Ntarget, DevScalars *ds);
+    static void scale(gp5cu_plan *p, void *field, int comp, DevScalars *ds, bool from_sigma);
+    static void max_density(gp5cu_plan *p, const void *field);
+    static void convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128);
+    static int step(gp5cu_stepper *st, void *field);  // queue one step; returns launches
+    static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
+};
+
+void set_scalars(cudaStream_t s, DevScalars *ds);
+void build_axis_plan(gp5cu_plan *p, int d);
+
+}  // namespace gp5

@@ -1,0 +1,185 @@
+/*
+ * gp5cu.h - C ABI of the B200 (sm_100a) pseudo-spectral Gross-Pitaevskii stepper.
+ *
+ * Plain C: opaque handles, raw pointers and sizes, int status codes.  Every field is a
+ * complex array of shape (nx, ny, nz, ncomp) in ColMajor order (x fastest, component
+ * slowest), interleaved (re, im): the layout of the reference's
+ * tensor_t = Eigen::Tensor<std::complex<double>,4> (src/traits.h:20) and of the numpy
+ * F-order view that gpCpp hands to Python (src/pyTools.h:93-104).  Precision GP5_C128
+ * stores complex128 (double2), GP5_C64 stores complex64 (float2); reductions are FP64 in
+ * both.
+ *
+ * Device pointers ("d" prefix) must come from cudaMalloc (or gp5cu_field_alloc, or a torch
+ * tensor) on the plan's device and be 16-byte aligned.  All work is queued on the plan's
+ * stream; calls that return host scalars synchronise that stream.  Calls on one plan (and
+ * on its functionals/steppers) are not thread-safe; distinct plans are independent.
+ *
+ * Each entry point names the reference interface it replaces (file:line in
+ * lucaparisi91/GP5).
+ */
+#ifndef GP5CU_H
+#define GP5CU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference throws std::runtime_error; gpCpp rethrows these) ---- */
+#define GP5_OK 0
+#define GP5_ERR_ARG 1         /* invalid argument (shape, pointer, kind, size) */
+#define GP5_ERR_CUDA 2        /* a CUDA runtime call failed; see gp5cu_last_error */
+#define GP5_ERR_NONFINITE 3   /* a reduction met NaN/Inf (norm blow-up) */
+#define GP5_ERR_TIMEOUT 4     /* a bounded device wait ran out */
+#define GP5_ERR_UNSUPPORTED 5 /* size/radix/feature not supported */
+#define GP5_ERR_STATE 6       /* object used in the wrong state */
+#define GP5_ERR_NOMEM 7       /* device allocation failed */
+
+/* ---- enums ---- */
+#define GP5_C128 0 /* complex128 bulk arithmetic */
+#define GP5_C64 1  /* complex64 bulk arithmetic, FP64 reductions */
+
+#define GP5_FORWARD (-1) /* e^{-2 pi i jk/n}, FFTW_FORWARD */
+#define GP5_BACKWARD 1   /* e^{+2 pi i jk/n}, FFTW_BACKWARD, unnormalised */
+
+#define GP5_FUNC_GP 0           /* gpFunctional (src/functional.cpp:13-102) */
+#define GP5_FUNC_LHY 1          /* LHYDropletFunctional (src/functional.cpp:105-122) */
+#define GP5_FUNC_LHY_UNLOCKED 2 /* LHYDropletUnlockedFunctional (src/functional.cpp:125-150) */
+
+#define GP5_POT_NONE 0
+#define GP5_POT_HARMONIC 1 /* harmonicPotential (src/externalPotential.cpp:11-32) */
+#define GP5_POT_ARRAY 2    /* potentialFromFile / sumPotential: caller's real array */
+
+#define GP5_STEP_EULER 0 /* euleroStepper (src/stepper.cpp:30-44) */
+#define GP5_STEP_RK4 1   /* RK4Stepper (src/stepper.cpp:46-82) */
+
+typedef struct gp5cu_plan gp5cu_plan;
+typedef struct gp5cu_functional gp5cu_functional;
+typedef struct gp5cu_stepper gp5cu_stepper;
+
+/* Library version (major*10000 + minor*100 + patch) and a message for a status code. */
+int gp5cu_version(void);
+const char *gp5cu_status_string(int status);
+/* Last error message recorded on this thread (empty when none). */
+const char *gp5cu_last_error(void);
+
+/* ---- discretisation + FFT plan ----------------------------------------------------------
+ * Replaces fourierTransformCreator::create (src/fourierTransform.cpp:227-249), the
+ * fftwFourierTransform constructor/plan (src/fourierTransform.cpp:129-181) and
+ * createUniformDiscretization for one rank (src/geometry.cpp:56-105).  shape = {nx,ny,nz};
+ * left/right = domain corners (gp::domain, src/geometry.h:41-65).  Any axis length in
+ * [2, 4096] whose prime factors are <= 61 is accepted.  device = CUDA ordinal. */
+int gp5cu_plan_create(gp5cu_plan **out, const int shape[3], const double left[3],
+                      const double right[3], int ncomp, int precision, int device);
+int gp5cu_plan_destroy(gp5cu_plan *plan);
+/* Queue all subsequent work of this plan on a caller stream (cudaStream_t); NULL = the
+ * plan's own stream. */
+int gp5cu_plan_set_stream(gp5cu_plan *plan, void *cuda_stream);
+int gp5cu_plan_synchronize(gp5cu_plan *plan);
+/* Bytes of one field (nx*ny*nz*ncomp complex elements of the plan's precision). */
+size_t gp5cu_field_bytes(const gp5cu_plan *plan);
+int gp5cu_field_alloc(gp5cu_plan *plan, void **dfield);
+int gp5cu_field_free(gp5cu_plan *plan, void *dfield);
+/* Host <-> device copies of one field in the plan precision (field::setTensor /
+ * field::getTensor, src/gpCpp.cpp:97-102; pyTools.h:12-56,68-105). */
+int gp5cu_upload(gp5cu_plan *plan, void *dfield, const void *host);
+int gp5cu_download(gp5cu_plan *plan, const void *dfield, void *host);
+/* Complex128 host data into a plan of either precision (converts on the device). */
+int gp5cu_upload_c128(gp5cu_plan *plan, void *dfield, const double *host_c128);
+int gp5cu_download_c128(gp5cu_plan *plan, const void *dfield, double *host_c128);
+
+/* ---- transforms and operators -------------------------------------------------------- */
+/* fourierTransform::apply(src, dst, FORWARD|BACKWARD) (src/fourierTransform.h:23;
+ * fftwFourierTransform::apply src/fourierTransform.cpp:184-214): unnormalised 3D C2C of
+ * every component, k-space in natural order.  src == dst is allowed. */
+int gp5cu_fft(gp5cu_plan *plan, const void *dsrc, void *ddst, int direction);
+/* operators::laplacian::apply (src/operators.cpp:28-36): dst = IFFT(-K^2 FFT(src)) / N^3. */
+int gp5cu_laplacian(gp5cu_plan *plan, const void *dsrc, void *ddst);
+/* gp::norm (src/geometry.cpp:190-214): dV * sum |psi_c|^2, FP64. */
+int gp5cu_norm(gp5cu_plan *plan, const void *dfield, int comp, double *out);
+/* gp::normalize (src/geometry.cpp:217-229): psi_c *= sqrt(N / norm_c). */
+int gp5cu_normalize(gp5cu_plan *plan, void *dfield, int comp, double N);
+/* gp.maxDensity (python/gp/gp.py:210-222): max |psi|^2 over all sites and components. */
+int gp5cu_max_density(gp5cu_plan *plan, const void *dfield, double *out);
+
+/* ---- functionals ---------------------------------------------------------------------- */
+typedef struct gp5cu_functional_desc {
+    int kind;              /* GP5_FUNC_* */
+    int has_couplings;     /* gpFunctional::setCouplings was called (functional.h:59) */
+    double couplings[4];   /* g(i,j) at [i*2+j]; 1 component uses [0] */
+    double masses[2];      /* gpFunctional::setMasses (default 1) */
+    double c3, c4;         /* LHY: H = -1/2 lap + (c3 n + c4 n^{3/2}); reference -3, 5/2 */
+    double alpha, beta, eta; /* unlocked LHY constants */
+    int potential;         /* GP5_POT_* */
+    double omegas[2][3];   /* harmonic trap frequencies per component */
+    const void *dpotential; /* GP5_POT_ARRAY: real array (nx,ny,nz,ncomp), double for
+                               GP5_C128 / float for GP5_C64, device memory, not copied */
+} gp5cu_functional_desc;
+
+/* Fills the reference defaults: LHY, c3 = -3, c4 = 5/2, masses 1, no potential. */
+void gp5cu_functional_desc_init(gp5cu_functional_desc *desc);
+/* functionalConstructor::create (src/functional.cpp:154-258) and the gpCpp LHY model
+ * (src/gpCpp.cpp:151-199). */
+int gp5cu_functional_create(gp5cu_plan *plan, const gp5cu_functional_desc *desc,
+                            gp5cu_functional **out);
+int gp5cu_functional_destroy(gp5cu_functional *func);
+/* functional::apply(old, new, t) (src/functional.h:15; model::apply src/gpCpp.cpp:167-171):
+ * dst = H src.  src != dst. */
+int gp5cu_apply_H(gp5cu_functional *func, const void *dsrc, void *ddst);
+
+typedef struct gp5cu_observables_t {
+    double norm;     /* dV sum |psi|^2 (all components) */
+    double energy;   /* E = ekin + epot + eint */
+    double ekin;     /* dV Re sum conj(psi) T psi, T = -1/2 (1/m) lap */
+    double epot;     /* dV sum V |psi|^2 */
+    double eint;     /* dV sum e_int(n); GP (g/2) n^2, LHY (c3/2) n^2 + (2 c4/5) n^{5/2} */
+    double mu;       /* Re <psi|H psi> / <psi|psi> */
+    double residual; /* ||H psi - mu psi|| / ||psi|| */
+} gp5cu_observables_t;
+/* Energy, chemical potential and residual (no reference counterpart: the reference only
+ * estimates mu from the norm decay, python/test/regressionTests/LHY_imaginary.py:48). */
+int gp5cu_observables(gp5cu_functional *func, const void *dfield, gp5cu_observables_t *out);
+
+/* ---- steppers ------------------------------------------------------------------------
+ * timeStepper (src/gpCpp.cpp:202-287) over euleroStepper / RK4Stepper
+ * (src/stepper.cpp:30-82).  imaginary != 0: time step (dt, 0); else (0, dt)
+ * (src/gpCpp.cpp:217-224). */
+int gp5cu_stepper_create(gp5cu_functional *func, int kind, double dt, int imaginary,
+                         gp5cu_stepper **out);
+int gp5cu_stepper_destroy(gp5cu_stepper *st);
+/* timeStepper::setRenormalization / unsetRenormalization (src/gpCpp.cpp:243-253); n = 0
+ * disables.  N[c] = target norm of component c. */
+int gp5cu_stepper_set_renormalization(gp5cu_stepper *st, int n, const double *N);
+/* phaseConstraint (src/constraint.cpp:6-17): psi <- |psi| e^{i phi} after each step;
+ * dphase = real array (nx,ny,nz,ncomp) in the plan precision, device memory; NULL = the
+ * nullConstraint (src/constraint.h:15-21). */
+int gp5cu_stepper_set_phase_constraint(gp5cu_stepper *st, const void *dphase);
+/* timeStepper::advance(field, nSteps) (src/gpCpp.cpp:255-269): nsteps steps in place on a
+ * device field; t += dt per step.  The step sequence is replayed from a CUDA graph. */
+int gp5cu_stepper_advance(gp5cu_stepper *st, void *dfield, int nsteps);
+/* timeStepper::getTime (src/gpCpp.cpp:273). */
+int gp5cu_stepper_get_time(const gp5cu_stepper *st, double *t);
+int gp5cu_stepper_set_time(gp5cu_stepper *st, double t);
+/* Host-buffer form of advance for callers that keep the field in host memory (the
+ * reference's Eigen tensor): upload, nsteps steps, download, on the plan stream.
+ * host_in and host_out may alias. */
+int gp5cu_stepper_advance_host(gp5cu_stepper *st, const void *host_in, void *host_out,
+                               int nsteps);
+/* Kernel launches one step issues (for launch accounting). */
+int gp5cu_stepper_launches_per_step(const gp5cu_stepper *st);
+/* Diagnostics (no reference counterpart; the reference's "step"/"FFT" timers,
+ * src/timers.h:112-113, are its nearest analogue): runs nrep eager steps with a CUDA event
+ * after every kernel launch and returns the mean duration of each launch of one step in
+ * ms[i] (milliseconds) with its kind in kinds[i] (axis*10 + mode: mode 0 forward, 1 inverse,
+ * 2 forward*K^2*inverse; 90 = point-wise kernel).  *nlaunch = launches per step; at most cap
+ * entries are written. */
+int gp5cu_stepper_profile(gp5cu_stepper *st, void *dfield, int nrep, double *ms, int *kinds, int cap,
+                          int *nlaunch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GP5CU_H */

@@ -1,0 +1,42 @@
+"""CPU checks of the C ABI library: it loads, exports every function include/gp5cu.h
+declares, and reports errors as status codes (no device work is attempted here)."""
+import ctypes
+
+from gp5_b200 import _abi
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(_abi.LIB_PATH)
+    names = _abi.header_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_version_status_strings_and_defaults():
+    L = _abi.lib()
+    assert L.gp5cu_version() >= 10000
+    assert L.gp5cu_status_string(0) == b"ok"
+    assert L.gp5cu_status_string(3).startswith(b"non-finite")
+    d = _abi.FunctionalDesc()
+    L.gp5cu_functional_desc_init(ctypes.byref(d))
+    # reference defaults: LHY constants -3 and 5/2 (functional.cpp:118), unit masses
+    assert d.kind == _abi.GP5_FUNC_LHY and d.c3 == -3.0 and d.c4 == 2.5
+    assert list(d.masses) == [1.0, 1.0] and d.potential == _abi.GP5_POT_NONE
+
+
+def test_argument_errors_without_device():
+    L = _abi.lib()
+    # NULL out pointer and bad arguments are rejected before any CUDA call
+    rc = L.gp5cu_plan_create(None, (ctypes.c_int * 3)(8, 8, 8), (ctypes.c_double * 3)(-1, -1, -1),
+                             (ctypes.c_double * 3)(1, 1, 1), 1, 0, 0)
+    assert rc == _abi.GP5_ERR_ARG
+    h = ctypes.c_void_p()
+    rc = L.gp5cu_plan_create(ctypes.byref(h), (ctypes.c_int * 3)(8, 8, 8), (ctypes.c_double * 3)(-1, -1, -1),
+                             (ctypes.c_double * 3)(1, 1, 1), 3, 0, 0)
+    assert rc == _abi.GP5_ERR_ARG and b"ncomp" in L.gp5cu_last_error()
+    rc = L.gp5cu_plan_create(ctypes.byref(h), (ctypes.c_int * 3)(8, 1, 8), (ctypes.c_double * 3)(-1, -1, -1),
+                             (ctypes.c_double * 3)(1, 1, 1), 1, 0, 0)
+    assert rc == _abi.GP5_ERR_ARG
+    rc = L.gp5cu_stepper_advance(None, None, 1)
+    assert rc == _abi.GP5_ERR_ARG

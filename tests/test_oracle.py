@@ -1,0 +1,128 @@
+"""CPU checks of the oracle against the reference's own known answers.
+
+Each test restates one of the reference's tests (lucaparisi91/GP5) on the oracle:
+  fft_test.cpp:10-83    forward/backward round trip, TOL 1e-6 (traits.h:46)
+  fft_test.cpp:85-153   spectral Laplacian of a Gaussian against the analytic value, 1e-6
+  test.py:92-119        LHY H applied to exp(-r^2) against the analytic value, 1e-4
+  test.py:123-147       normalise to 1
+  test.py:10-69         geometry: space steps, cell-centred grid
+plus the long-double direct DFT (oracle/dft_ld.c) pinning numpy's FFT on small grids.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import gp_oracle as o
+from oracle import dft3_ld
+
+
+def test_geometry_space_step_and_grid():
+    geo = o.Geometry((100, 200, 50))  # test.py:10-18 (default box [-1, 1])
+    assert geo.left == (-1, -1, -1) and geo.right == (1, 1, 1)
+    assert geo.space_step(0) == 2 / 100 and geo.space_step(1) == 2 / 200 and geo.space_step(2) == 2 / 50
+    X, Y, Z = o.grid(geo)  # test.py:35-40
+    assert abs(X.min() - (geo.left[0] + geo.space_step(0) / 2)) < 1e-12
+    assert abs(X.max() - (geo.right[0] - geo.space_step(0) / 2)) < 1e-12
+    assert abs((X[1, 0, 0] - X[0, 0, 0]) - geo.space_step(0)) < 1e-12
+
+
+def test_momentum_conventions():
+    # even n: Nyquist -> -n/2 ; odd n: i <= (n-1)/2 positive (geometry.cpp:127-148)
+    geo = o.Geometry((8, 7, 2), (0, 0, 0), (2 * math.pi, 2 * math.pi, 2 * math.pi))
+    assert list(o.momentum_axis(geo, 0)) == [0, 1, 2, 3, -4, -3, -2, -1]
+    assert list(o.momentum_axis(geo, 1)) == [0, 1, 2, 3, -3, -2, -1]
+
+
+@pytest.mark.parametrize("shape", [(6, 10, 12), (8, 8, 8), (5, 7, 3), (30, 4, 2)])
+def test_numpy_fft_matches_long_double_dft(shape):
+    rng = np.random.default_rng(1)
+    a = (rng.standard_normal(shape + (1,)) + 1j * rng.standard_normal(shape + (1,)))
+    for direction in (o.FORWARD, o.BACKWARD):
+        ref = dft3_ld(a, direction)
+        got = o.fft3(a, direction)
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-14
+
+
+def test_fft_forward_backward_roundtrip():
+    # fft_test.cpp:10-83: N=(50,170,150), box [-1/2,1/2]^3, Gaussian sigma=(1,0.5,0.2)
+    geo = o.Geometry((50, 170, 150), (-0.5,) * 3, (0.5,) * 3)
+    f = o.new_field(geo)
+    o.init_gaussian(geo, (1, 0.5, 0.2), f)
+    back = o.fft3(o.fft3(f, o.FORWARD), o.BACKWARD) * (1.0 / geo.n_sites)
+    assert np.max(np.abs(back - f)) < 1e-6
+
+
+def test_laplacian_of_gaussian_analytic():
+    # fft_test.cpp:85-153: N=(300,250,77), sigma=0.05, max |L - analytic| <= 1e-6
+    geo = o.Geometry((300, 250, 77), (-0.5,) * 3, (0.5,) * 3)
+    f = o.new_field(geo)
+    sigma = 0.05
+    o.init_gaussian(geo, sigma, f)
+    lap = o.laplacian(f, geo)[..., 0]
+    X, Y, Z = o.grid(geo)
+    R2 = X * X + Y * Y + Z * Z
+    alpha = 1 / (2 * sigma * sigma)
+    L2 = np.exp(-alpha * R2) * (-R2 * alpha * 2 + 3) * (-2) * alpha
+    assert np.max(np.abs(L2 - lap)) <= 1e-6
+
+
+def test_lhy_apply_gaussian_analytic():
+    # test.py:92-119: 100^3, box [-4,4]^3, psi = exp(-r^2)
+    geo = o.Geometry((100, 100, 100), (-4,) * 3, (4,) * 3)
+    X, Y, Z = o.grid(geo)
+    r2 = X * X + Y * Y + Z * Z
+    psi = o.new_field(geo)
+    psi[..., 0] = np.exp(-r2) + 0j
+    out = o.Functional("lhy").apply(psi, geo)[..., 0]
+    p = np.exp(-r2)
+    expected = (3 - 2 * r2) * p + (-3 * p ** 2 + 5 / 2 * p ** 3) * p
+    assert np.max(np.abs(expected - out.real)) < 1e-4
+
+
+def test_renormalize():
+    # test.py:123-147
+    geo = o.Geometry((50, 50, 50), (-5,) * 3, (5,) * 3)
+    X, Y, Z = o.grid(geo)
+    psi = o.new_field(geo)
+    psi[..., 0] = np.exp(-(X * X + Y * Y + Z * Z))
+    o.normalize(1, psi, 0, geo)
+    assert abs(o.norm(psi, 0, geo) - 1) < 1e-12
+
+
+def test_rk4_euler_consistency_small_dt():
+    # one RK4 step and 16 Euler steps of dt/16 agree to O(dt^2) for a smooth state
+    geo = o.Geometry((12, 12, 12), (-4,) * 3, (4,) * 3)
+    psi = o.gaussian_with_noise(geo, 1.0, 0.0, seed=0, N=1.0)
+    f = o.Functional("gp", couplings=[[1.0]], V=o.harmonic_potential(geo, [(1, 1, 1)]))
+    rk = o.Stepper(f, geo, 1e-3, "RK4", True).advance(psi.copy(), 1)
+    eu = o.Stepper(f, geo, 1e-3 / 16, "eulero", True).advance(psi.copy(), 16)
+    assert np.max(np.abs(rk - eu)) / np.max(np.abs(rk)) < 1e-4
+
+
+def test_energy_definitions_consistent():
+    # E(psi) derivative along psi equals 2 Re<psi|H psi> (e_int' = f) for LHY and GP
+    geo = o.Geometry((16, 16, 16), (-6,) * 3, (6,) * 3)
+    psi = o.gaussian_with_noise(geo, 1.5, 1e-3, seed=3, N=20.0, phase_noise=True)
+    for f in (o.Functional("lhy"),
+              o.Functional("gp", couplings=[[2.0]], V=o.harmonic_potential(geo, [(1, 0.5, 2)]))):
+        eps = 1e-6
+        Ep = o.observables(f, psi * (1 + eps), geo)["E"]
+        Em = o.observables(f, psi * (1 - eps), geo)["E"]
+        dE = (Ep - Em) / (2 * eps)
+        ob = o.observables(f, psi, geo)
+        assert abs(dE - 2 * ob["mu"] * ob["norm"]) / abs(dE) < 1e-6
+
+
+@pytest.mark.slow
+def test_lhy_mu_protocol_near_reference_golden():
+    """python/test/regressionTests/LHY_imaginary.py with its committed golden (mu file).
+
+    The committed script's protocol, restated exactly, converges to -0.38366638; the
+    committed number is -0.38372999.  The norm-decay estimator carries an O(dt) bias of
+    ~6.6e-4 (the converged state's <H>/N is -0.38432), and the golden sits 6.4e-5 away
+    from the restatement: it is pinned here to 1e-4, not bitwise.
+    """
+    mu, blocks, _ = o.lhy_mu_protocol()
+    assert abs(mu - (-0.3837299937094331)) < 1e-4
+    assert abs(mu - (-0.3836663826072363)) < 1e-12
