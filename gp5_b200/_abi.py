@@ -10,6 +10,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import re
+import weakref
 from typing import Optional, Sequence
 
 import numpy as np
@@ -139,6 +140,7 @@ class Plan:
         self.right = tuple(float(v) for v in right)
         self.ncomp = int(ncomp)
         self.precision = precision
+        self._children = weakref.WeakSet()
         h = C.c_void_p()
         check(lib().gp5cu_plan_create(C.byref(h), (C.c_int * 3)(*self.shape), (C.c_double * 3)(*self.left),
                                       (C.c_double * 3)(*self.right), self.ncomp, precision, device))
@@ -188,7 +190,10 @@ class Plan:
         check(lib().gp5cu_plan_set_stream(self.h, C.c_void_p(stream_handle or None)))
 
     def close(self):
+        # children (fields, functionals, steppers) go first: their handles refer to the plan
         if getattr(self, "h", None):
+            for c in sorted(list(self._children), key=lambda c: -c._order):
+                c.close()
             lib().gp5cu_plan_destroy(self.h)
             self.h = None
 
@@ -202,11 +207,14 @@ class Plan:
 class DeviceField:
     """One field (nx, ny, nz, ncomp) in device memory, allocated by the library."""
 
+    _order = 0
+
     def __init__(self, plan: Plan):
         self.plan = plan
         p = C.c_void_p()
         check(lib().gp5cu_field_alloc(plan.h, C.byref(p)))
         self.ptr = p
+        plan._children.add(self)
 
     def upload(self, host: np.ndarray) -> None:
         a = np.asarray(host)
@@ -231,7 +239,7 @@ class DeviceField:
     def close(self):
         if getattr(self, "ptr", None) and getattr(self.plan, "h", None):
             lib().gp5cu_field_free(self.plan.h, self.ptr)
-            self.ptr = None
+        self.ptr = None
 
     def __del__(self):
         try:
@@ -241,6 +249,8 @@ class DeviceField:
 
 
 class Functional:
+    _order = 1
+
     def __init__(self, plan: Plan, kind: int = GP5_FUNC_LHY, couplings=None, masses=None, c3=-3.0, c4=2.5,
                  alpha=0.0, beta=0.0, eta=0.0, omegas=None, potential: Optional[DeviceField] = None,
                  potential_ptr: Optional[int] = None):
@@ -272,6 +282,7 @@ class Functional:
         h = C.c_void_p()
         check(lib().gp5cu_functional_create(plan.h, C.byref(d), C.byref(h)))
         self.h = h
+        plan._children.add(self)
 
     def apply(self, src: DeviceField, dst: DeviceField) -> None:
         check(lib().gp5cu_apply_H(self.h, src.ptr, dst.ptr))
@@ -282,9 +293,10 @@ class Functional:
         return o.as_dict()
 
     def close(self):
-        if getattr(self, "h", None):
+        # a plan that is already gone took the functional's memory with it
+        if getattr(self, "h", None) and getattr(self.plan, "h", None):
             lib().gp5cu_functional_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -294,12 +306,15 @@ class Functional:
 
 
 class Stepper:
+    _order = 2
+
     def __init__(self, func: Functional, dt: float, kind: int = GP5_STEP_RK4, imaginary: bool = True):
         self.func = func
         self.dt = float(dt)
         h = C.c_void_p()
         check(lib().gp5cu_stepper_create(func.h, kind, self.dt, 1 if imaginary else 0, C.byref(h)))
         self.h = h
+        func.plan._children.add(self)
 
     def set_renormalization(self, N: Optional[Sequence[float]]) -> None:
         if N is None:
@@ -338,9 +353,9 @@ class Stepper:
         return int(lib().gp5cu_stepper_launches_per_step(self.h))
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self.func.plan, "h", None):
             lib().gp5cu_stepper_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

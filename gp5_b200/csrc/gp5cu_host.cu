@@ -5,7 +5,10 @@
 // is kept per thread for gp5cu_last_error().
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "plan.hpp"
@@ -29,6 +32,17 @@ __global__ void k_set_scalars(DevScalars *ds) {
     ds->sigma[0] = ds->sigma[1] = 1.0;
     ds->alpha[0] = ds->alpha[1] = 1.0;
     ds->status = 0u;
+}
+
+void smem_opt_in(const void *kernel, size_t bytes, int dev) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> done;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &have = done[{kernel, dev}];
+    if (have >= bytes) return;
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+               "cudaFuncSetAttribute");
+    have = bytes;
 }
 
 void ProfRec::record(cudaStream_t s, int kind) {

@@ -48,13 +48,12 @@ inline TileGeom make_geom(const gp5cu_plan *p, int axis, int lines, bool pow2_bx
 
 inline RedSlot red_slot(const gp5cu_plan *p) { return RedSlot{p->partials, p->counter}; }
 
+// Opt a kernel in to more than 48 KB of dynamic shared memory, once per (kernel, device,
+// size); the bookkeeping is keyed by the kernel's address.
+void smem_opt_in(const void *kernel, size_t bytes, int dev);
+
 template <class K> inline void ensure_smem(K kernel, size_t bytes, int dev) {
-    static bool done[64] = {false};
-    if (bytes > 48 * 1024 && dev < 64 && !done[dev]) {
-        check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
-                   "cudaFuncSetAttribute");
-        done[dev] = true;
-    }
+    if (bytes > 48 * 1024) smem_opt_in((const void *)kernel, bytes, dev);
 }
 
 template <typename Real, int N, bool CONTIG, int MODE, class Op>
