@@ -209,8 +209,32 @@ __device__ __forceinline__ void reg_pass(V (&v)[RegCfg<N>::E], int tid, int line
         for (int r = 0; r < R; r++) x[r] = v[t + r * (E / R)];
         if constexpr (Ns > 1) {
             const int bm = b % Ns;
+            constexpr int step = N / (Ns * R);
+            if constexpr (R == 16) {
+                // w^r for r = 1..15 from four table entries (w, w^2, w^4, w^8); every power is
+                // a product of at most four exactly rounded table values (<= 3 extra roundings)
+                const V w1 = twiddle<DIR>(tw, bm * step), w2 = twiddle<DIR>(tw, 2 * bm * step);
+                const V w4 = twiddle<DIR>(tw, 4 * bm * step), w8 = twiddle<DIR>(tw, 8 * bm * step);
+                const V w3 = cmul(w2, w1), w12 = cmul(w8, w4);
+                x[1] = cmul(x[1], w1);
+                x[2] = cmul(x[2], w2);
+                x[3] = cmul(x[3], w3);
+                x[4] = cmul(x[4], w4);
+                x[5] = cmul(x[5], cmul(w4, w1));
+                x[6] = cmul(x[6], cmul(w4, w2));
+                x[7] = cmul(x[7], cmul(w4, w3));
+                x[8] = cmul(x[8], w8);
+                x[9] = cmul(x[9], cmul(w8, w1));
+                x[10] = cmul(x[10], cmul(w8, w2));
+                x[11] = cmul(x[11], cmul(w8, w3));
+                x[12] = cmul(x[12], w12);
+                x[13] = cmul(x[13], cmul(w12, w1));
+                x[14] = cmul(x[14], cmul(w12, w2));
+                x[15] = cmul(x[15], cmul(w12, w3));
+            } else {
 #pragma unroll
-            for (int r = 1; r < R; r++) x[r] = cmul(x[r], twiddle<DIR>(tw, r * bm * (N / (Ns * R))));
+                for (int r = 1; r < R; r++) x[r] = cmul(x[r], twiddle<DIR>(tw, r * bm * step));
+            }
         }
         dft_r<R, DIR>(x);
         if constexpr (last) {

@@ -45,6 +45,20 @@ void smem_opt_in(const void *kernel, size_t bytes, int dev) {
     have = bytes;
 }
 
+int resident_blocks(const void *kernel, int threads, size_t smem, int dev) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find({kernel, dev});
+    if (it != cache.end()) return it->second;
+    int nb = 0;
+    check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (nb < 1) nb = 1;
+    cache[{kernel, dev}] = nb;
+    return nb;
+}
+
 void ProfRec::record(cudaStream_t s, int kind) {
     if (idx >= ev.size()) {
         cudaEvent_t e;
@@ -222,6 +236,7 @@ int gp5cu_plan_create(gp5cu_plan **out, const int shape[3], const double left[3]
             // (geometry.cpp:108-152); tabulated squared, as K*K in operators.cpp:20.
             const int n = shape[d];
             const double delta = 2 * M_PI / (right[d] - left[d]);
+            p->dk[d] = delta;
             std::vector<double> k2(n);
             p->pos_host[d].resize(n);
             const double dx = (right[d] - left[d]) / n;
@@ -239,6 +254,7 @@ int gp5cu_plan_create(gp5cu_plan **out, const int shape[3], const double left[3]
         // partial-sum slots: the largest grid any kernel of this plan launches
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        p->sms = sms;
         p->pw_blocks = sms * 8;
         long long mb = p->pw_blocks;
         for (int d = 0; d < 3; d++) {

@@ -28,6 +28,7 @@ inline TileGeom make_geom(const gp5cu_plan *p, int axis, int lines, bool pow2_bx
         g.tiles_x = 1;
         g.n_other = (long long)g.ny * g.nz * g.nc;
         *tiles = (g.n_other + lines - 1) / lines;
+        g.ntiles = *tiles;
     } else {
         int bx = std::min(lines, g.nx);
         if (pow2_bx) {
@@ -42,6 +43,7 @@ inline TileGeom make_geom(const gp5cu_plan *p, int axis, int lines, bool pow2_bx
         g.tiles_x = (g.nx + bx - 1) / bx;
         g.n_other = axis == 1 ? (long long)g.nz * g.nc : (long long)g.ny * g.nc;
         *tiles = (long long)g.tiles_x * ((g.n_other + bo - 1) / bo);
+        g.ntiles = *tiles;
     }
     return g;
 }
@@ -51,6 +53,9 @@ inline RedSlot red_slot(const gp5cu_plan *p) { return RedSlot{p->partials, p->co
 // Opt a kernel in to more than 48 KB of dynamic shared memory, once per (kernel, device,
 // size); the bookkeeping is keyed by the kernel's address.
 void smem_opt_in(const void *kernel, size_t bytes, int dev);
+
+// CTAs of a kernel resident per SM (cached per kernel and device).
+int resident_blocks(const void *kernel, int threads, size_t smem, int dev);
 
 template <class K> inline void ensure_smem(K kernel, size_t bytes, int dev) {
     if (bytes > 48 * 1024) smem_opt_in((const void *)kernel, bytes, dev);
@@ -175,7 +180,7 @@ static void kinetic_passes(gp5cu_plan *p, const void *src, void *w, double coef0
     launch_axis<Real, true, MODE_FWD>(p, 0, in);
     OpCopy<Real> cp{(const V *)w, (V *)w};
     launch_axis<Real, false, MODE_FWD>(p, 1, cp);
-    OpKinetic<Real> kin{(const V *)w, (V *)w, p->k2[0], p->k2[1], p->k2[2], coef0, coef1};
+    OpKinetic<Real> kin{(const V *)w, (V *)w, p->k2[0], p->k2[1], p->k2[2], coef0, coef1, p->shape[2], p->dk[2]};
     launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
     launch_axis<Real, false, MODE_INV>(p, 1, cp);
 }
@@ -327,7 +332,7 @@ template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) 
         }
         OpCopy<Real> cp{W, W};
         launch_axis<Real, false, MODE_FWD>(p, 1, cp);
-        OpKinetic<Real> kin{W, W, p->k2[0], p->k2[1], p->k2[2], f->coef[0], f->coef[1]};
+        OpKinetic<Real> kin{W, W, p->k2[0], p->k2[1], p->k2[2], f->coef[0], f->coef[1], p->shape[2], p->dk[2]};
         launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
         launch_axis<Real, false, MODE_INV>(p, 1, cp);
         launches += 4;

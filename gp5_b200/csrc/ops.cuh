@@ -31,40 +31,60 @@ struct DevScalars {
 };
 
 // ---- plain copy / kinetic-multiply ops --------------------------------------------------
+// Hook interface of the axis passes:
+//   load(g, e, acc)          value entering the transform at element g (prologue)
+//   mid(v, e)                k-space multiply between a forward and an inverse transform
+//   pre(g) -> Pre            operand loads of the epilogue (issued BATCH elements at a time)
+//   post(g, e, v, pre, acc)  epilogue: consume the transformed value and store
+//   streams(p)               arrays the pass reads, for the L2 prefetch of the next tile
+//   finalize(sums)           last block, with the FP64 sums of the NRED accumulators
+struct NoPre {};
+
 template <typename Real> struct OpCopy {
-    static constexpr int NRED = 0;
+    static constexpr int NRED = 0, BATCH = 1;
     using V = cpx<Real>;
+    using Pre = NoPre;
     const V *src;
     V *dst;
     __device__ __forceinline__ V load(long long g, const LineRef &, double *) const { return src[g]; }
     __device__ __forceinline__ V mid(V v, const LineRef &) const { return v; }
-    __device__ __forceinline__ void store(long long g, const LineRef &, V v, double *) const { dst[g] = v; }
+    __device__ __forceinline__ Pre pre(long long) const { return Pre{}; }
+    __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &, double *) const { dst[g] = v; }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const { p[0] = src; return 1; }
     __device__ __forceinline__ void finalize(const double *) const {}
 };
 
 // z pass of an H application: forward z, times (K^2 * coef_c), inverse z.
 template <typename Real> struct OpKinetic {
-    static constexpr int NRED = 0;
+    static constexpr int NRED = 0, BATCH = 1;
     using V = cpx<Real>;
+    using Pre = NoPre;
     const V *src;
     V *dst;
     const double *kx2, *ky2, *kz2;  // k_d^2 tables
     double coef0, coef1;            // per component: 1/(2 m N^3) for H, -1/N^3 for the Laplacian
+    int nz;                         // k_z is formed arithmetically (same value as the table):
+    double dkz;                     // k = dkz * m, m = k < nz/2 (even) or k <= (nz-1)/2 (odd), else k - nz
     __device__ __forceinline__ V load(long long g, const LineRef &, double *) const { return src[g]; }
     __device__ __forceinline__ V mid(V v, const LineRef &e) const {
-        const double k2 = (__ldg(kx2 + e.i) + __ldg(ky2 + e.j)) + __ldg(kz2 + e.k);
+        const int half = (nz % 2 == 0) ? nz / 2 : (nz - 1) / 2 + 1;
+        const double kz = e.k < half ? dkz * e.k : (-nz + e.k) * dkz;
+        const double k2 = (__ldg(kx2 + e.i) + __ldg(ky2 + e.j)) + kz * kz;
         const Real f = (Real)(k2 * (e.c ? coef1 : coef0));
         return cscale(v, f);
     }
-    __device__ __forceinline__ void store(long long g, const LineRef &, V v, double *) const { dst[g] = v; }
+    __device__ __forceinline__ Pre pre(long long) const { return Pre{}; }
+    __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &, double *) const { dst[g] = v; }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const { p[0] = src; return 1; }
     __device__ __forceinline__ void finalize(const double *) const {}
 };
 
 // ---- stage input (prologue of the first forward pass) -----------------------------------
 // u~ = sigma_c psi - c kprev ; optional sum |u~|^2 per component -> alpha_c = sqrt(N_c/(dV S)).
 template <typename Real, bool RED> struct OpStageIn {
-    static constexpr int NRED = RED ? 2 : 0;
+    static constexpr int NRED = RED ? 2 : 0, BATCH = 1;
     using V = cpx<Real>;
+    using Pre = NoPre;
     const V *psi;
     const V *kprev;  // null for the first stage
     V *dst;
@@ -90,7 +110,13 @@ template <typename Real, bool RED> struct OpStageIn {
         return p;
     }
     __device__ __forceinline__ V mid(V v, const LineRef &) const { return v; }
-    __device__ __forceinline__ void store(long long g, const LineRef &, V v, double *) const { dst[g] = v; }
+    __device__ __forceinline__ Pre pre(long long) const { return Pre{}; }
+    __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &, double *) const { dst[g] = v; }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const {
+        p[0] = psi;
+        if (kprev) { p[1] = kprev; return 2; }
+        return 1;
+    }
     __device__ __forceinline__ void finalize(const double *s) const {
         if (RED) {
             ds->alpha[0] = sqrt(Nt0 / (dV * s[0]));
@@ -217,17 +243,31 @@ __device__ __forceinline__ double interaction_energy(const EpiParams<Real> &P, c
 }
 
 // The epilogue of one site: t[c] = kinetic of u~_c (already times 1/(2 m N^3) K^2).
+// Operands of one site's epilogue, loaded before any store of the batch.
+template <typename Real> struct EpiIn {
+    cpx<Real> psi, kprev, kacc;
+};
+
+template <typename Real>
+__device__ __forceinline__ EpiIn<Real> epi_load(const EpiParams<Real> &P, long long g) {
+    EpiIn<Real> in;
+    in.psi = P.psi[g];
+    in.kprev = P.mode >= EPI_RK2 ? P.kprev[g] : mk<Real>(0, 0);
+    in.kacc = (P.mode == EPI_RK3 || P.mode == EPI_RK4) ? P.kacc[g] : mk<Real>(0, 0);
+    return in;
+}
+
 template <typename Real, int NC, bool RED>
 __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long long s, int i, int j, int k,
-                                              const cpx<Real> (&t)[NC], double *acc) {
+                                              const cpx<Real> (&t)[NC], const EpiIn<Real> (&in)[NC],
+                                              double *acc) {
     using V = cpx<Real>;
     V p[NC], u[NC], kin[NC], h[NC];
     Real Vv[NC], nn[NC];
     const int mode = P.mode;
 #pragma unroll
     for (int c = 0; c < NC; c++) {
-        const long long g = s + (long long)c * P.nsites;
-        V x = P.psi[g];
+        V x = in[c].psi;
         if (P.use_sigma) x = cscale(x, (Real)__ldg(&P.ds->sigma[c]));
         p[c] = x;
         V ut = x;
@@ -235,7 +275,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long lon
             V c0;
             c0.x = P.cre;
             c0.y = P.cim;
-            ut = csub(x, cmul(c0, P.kprev[g]));
+            ut = csub(x, cmul(c0, in[c].kprev));
         }
         if (P.use_alpha) {
             const Real a = (Real)__ldg(&P.ds->alpha[c]);
@@ -273,9 +313,8 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long lon
 #pragma unroll
         for (int c = 0; c < NC; c++) {
             const long long g = s + (long long)c * P.nsites;
-            const V k1 = P.kprev[g];
             P.kout[g] = h[c];
-            P.kacc[g] = cadd(k1, cscale(h[c], (Real)2));
+            P.kacc[g] = cadd(in[c].kprev, cscale(h[c], (Real)2));
         }
         return;
     }
@@ -283,8 +322,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long lon
 #pragma unroll
         for (int c = 0; c < NC; c++) {
             const long long g = s + (long long)c * P.nsites;
-            const V a = P.kacc[g];
-            P.kacc[g] = cadd(a, cscale(h[c], (Real)2));
+            P.kacc[g] = cadd(in[c].kacc, cscale(h[c], (Real)2));
             P.kout[g] = h[c];
         }
         return;
@@ -297,7 +335,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long lon
     for (int c = 0; c < NC; c++) {
         const long long g = s + (long long)c * P.nsites;
         V sum = h[c];
-        if (mode == EPI_RK4) sum = cadd(P.kacc[g], h[c]);
+        if (mode == EPI_RK4) sum = cadd(in[c].kacc, h[c]);
         V r = csub(p[c], cmul(d, sum));
         if (P.phase_exp) {
             const Real a = sqrt(r.x * r.x + r.y * r.y);
@@ -326,15 +364,26 @@ template <typename Real> struct EpiFinalize {
 
 // Fused epilogue (one component): the inverse x pass hands every element to the site logic.
 template <typename Real, bool RED> struct OpStageOut {
-    static constexpr int NRED = RED ? kNRed : 0;
+    static constexpr int NRED = RED ? kNRed : 0, BATCH = 2;
     using V = cpx<Real>;
+    using Pre = EpiIn<Real>;
     const V *src;  // inverse-pass input buffer
     EpiParams<Real> P;
     __device__ __forceinline__ V load(long long g, const LineRef &, double *) const { return src[g]; }
     __device__ __forceinline__ V mid(V v, const LineRef &) const { return v; }
-    __device__ __forceinline__ void store(long long g, const LineRef &e, V v, double *acc) const {
+    __device__ __forceinline__ Pre pre(long long g) const { return epi_load(P, g); }
+    __device__ __forceinline__ void post(long long g, const LineRef &e, V v, const Pre &in, double *acc) const {
         const V t[1] = {v};
-        epilogue_site<Real, 1, RED>(P, g, e.i, e.j, e.k, t, acc);
+        const Pre ins[1] = {in};
+        epilogue_site<Real, 1, RED>(P, g, e.i, e.j, e.k, t, ins, acc);
+    }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const {
+        int n = 0;
+        p[n++] = src;
+        p[n++] = P.psi;
+        if (P.mode >= EPI_RK2) p[n++] = P.kprev;
+        if (P.mode == EPI_RK3 || P.mode == EPI_RK4) p[n++] = P.kacc;
+        return n;
     }
     __device__ __forceinline__ void finalize(const double *s) const { EpiFinalize<Real>::run(P, s); }
 };
@@ -346,12 +395,16 @@ template <typename Real, int NC, bool RED> struct OpSiteEpilogue {
     EpiParams<Real> P;
     __device__ __forceinline__ void site(long long s, double *acc) const {
         V t[NC];
+        EpiIn<Real> in[NC];
 #pragma unroll
-        for (int c = 0; c < NC; c++) t[c] = P.tsrc[s + (long long)c * P.nsites];
+        for (int c = 0; c < NC; c++) {
+            t[c] = P.tsrc[s + (long long)c * P.nsites];
+            in[c] = epi_load(P, s + (long long)c * P.nsites);
+        }
         const int i = (int)(s % P.nx);
         const long long r = s / P.nx;
         const int j = (int)(r % P.ny), k = (int)(r / P.ny);
-        epilogue_site<Real, NC, RED>(P, s, i, j, k, t, acc);
+        epilogue_site<Real, NC, RED>(P, s, i, j, k, t, in, acc);
     }
     __device__ __forceinline__ void finalize(const double *s) const { EpiFinalize<Real>::run(P, s); }
 };

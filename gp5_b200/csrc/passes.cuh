@@ -30,6 +30,7 @@ struct TileGeom {
     int bx, bo;         // strided tiles: consecutive x lines, other lines
     int tiles_x;        // strided tiles: ceil(nx / bx)
     long long n_other;  // strided: number of (other) line groups; x axis: total lines
+    long long ntiles;   // tiles of the pass (a persistent CTA walks tile += gridDim.x)
 };
 
 struct RedSlot {
@@ -158,18 +159,49 @@ __device__ void reduce_and_finalize(const double *acc_in, const RedSlot &rs, con
     }
 }
 
+// ---- L2 prefetch of a tile's input streams -------------------------------------------------
+// cp.async.bulk.prefetch.L2 brings a contiguous range into L2 without registers or shared
+// memory; a persistent CTA issues it for the tile it will process next, so that the DRAM
+// reads of that tile overlap the transform of the current one.  Ranges that are not 16-byte
+// aligned and sized are skipped (the prefetch is only a hint).
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
+    if ((((uintptr_t)p) & 15u) == 0 && (bytes & 15u) == 0 && bytes > 0)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// L2 prefetch of the auxiliary streams (every stream but the first, which the prologue loads
+// at once) of a contiguous x tile: one instruction per stream, issued by thread 0 at kernel
+// start, so that the epilogue's operand loads hit L2 while the transform runs.
+template <typename V, class Op>
+__device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, const Op &op) {
+    const void *st[4];
+    const int ns = op.streams(st);
+    if (ns < 2 || threadIdx.x != 0 || g.axis != 0) return;
+    const long long L0 = tile * g.lines;
+    long long L1 = L0 + g.lines;
+    if (L1 > g.n_other) L1 = g.n_other;
+    const long long e0 = L0 * g.nx, cnt = (L1 - L0) * g.nx;
+    for (int q = 1; q < ns; q++)
+        prefetch_l2(reinterpret_cast<const V *>(st[q]) + e0, (unsigned)(cnt * sizeof(V)));
+}
+
 // ---- register-engine kernel ----------------------------------------------------------------
-// Threads: LINES lines x T threads per line; 256 threads for every supported N.
+// Threads: LINES lines x T threads per line; 256 threads for every supported N; one tile per
+// CTA.
 template <int N> struct RegTile {
     static constexpr int T = RegCfgAll<N>::T;
     static constexpr int LINES = 256 / T;
 };
 
+template <typename Real> struct RegOcc { static constexpr int value = sizeof(Real) == 8 ? 2 : 3; };
+
 template <typename Real, int N, bool CONTIG, int MODE, class Op>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, RegOcc<Real>::value)
 k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedSlot rs) {
     using V = cpx<Real>;
     constexpr int E = RegCfg<N>::E, T = RegCfgAll<N>::T, LINES = RegTile<N>::LINES;
+    constexpr int NB = Op::BATCH;
+    static_assert(E % NB == 0, "batch must divide the elements per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *sm = reinterpret_cast<V *>(smem_raw);
 
@@ -177,59 +209,70 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
     if (CONTIG) { tid = threadIdx.x % T; line = threadIdx.x / T; }
     else { line = threadIdx.x % LINES; tid = threadIdx.x / LINES; }
 
-    LineRef lr = line_ref(g, blockIdx.x, line);
     double acc[Op::NRED > 0 ? Op::NRED : 1];
 #pragma unroll
     for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); r++) acc[r] = 0.0;
 
-    V v[E];
-#pragma unroll
-    for (int m = 0; m < E; m++) {
-        const int pos = tid + T * m;
-        if (lr.valid) {
-            LineRef e = lr;
-            set_pos(g, e, pos);
-            v[m] = op.load(lr.base + pos * g.estride, e, acc);
-        } else {
-            v[m] = mk<Real>(0, 0);
-        }
-    }
-    if constexpr (CONTIG) {
-        LayContig<N> lay;
-        if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
-        else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
-        if (MODE == MODE_FWD_MID_INV) {
-#pragma unroll
-            for (int m = 0; m < E; m++) {
-                LineRef e = lr;
-                set_pos(g, e, tid + T * m);
-                v[m] = op.mid(v[m], e);
-            }
-            __syncthreads();
-            reg_fft<N, 1>(v, tid, line, tw, sm, lay);
-        }
-    } else {
-        LayStrided lay{LINES};
-        if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
-        else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
-        if (MODE == MODE_FWD_MID_INV) {
-#pragma unroll
-            for (int m = 0; m < E; m++) {
-                LineRef e = lr;
-                set_pos(g, e, tid + T * m);
-                v[m] = op.mid(v[m], e);
-            }
-            __syncthreads();
-            reg_fft<N, 1>(v, tid, line, tw, sm, lay);
-        }
-    }
-    if (lr.valid) {
+    if (CONTIG) prefetch_aux<V>(g, blockIdx.x, op);
+    {
+        const long long tile = blockIdx.x;
+        LineRef lr = line_ref(g, tile, line);
+        V v[E];
 #pragma unroll
         for (int m = 0; m < E; m++) {
             const int pos = tid + T * m;
-            LineRef e = lr;
-            set_pos(g, e, pos);
-            op.store(lr.base + pos * g.estride, e, v[m], acc);
+            if (lr.valid) {
+                LineRef e = lr;
+                set_pos(g, e, pos);
+                v[m] = op.load(lr.base + pos * g.estride, e, acc);
+            } else {
+                v[m] = mk<Real>(0, 0);
+            }
+        }
+        if constexpr (CONTIG) {
+            LayContig<N> lay;
+            if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+            else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+            if (MODE == MODE_FWD_MID_INV) {
+#pragma unroll
+                for (int m = 0; m < E; m++) {
+                    LineRef e = lr;
+                    set_pos(g, e, tid + T * m);
+                    v[m] = op.mid(v[m], e);
+                }
+                __syncthreads();  // also a scheduling fence: keeps register pressure below 128
+                reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+            }
+        } else {
+            LayStrided lay{LINES};
+            if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+            else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+            if (MODE == MODE_FWD_MID_INV) {
+#pragma unroll
+                for (int m = 0; m < E; m++) {
+                    LineRef e = lr;
+                    set_pos(g, e, tid + T * m);
+                    v[m] = op.mid(v[m], e);
+                }
+                __syncthreads();  // also a scheduling fence: keeps register pressure below 128
+                reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+            }
+        }
+        if (lr.valid) {
+            // epilogue in batches: the operand loads of NB elements are issued together
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += NB) {
+                typename Op::Pre pre[NB];
+#pragma unroll
+                for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * g.estride);
+#pragma unroll
+                for (int j = 0; j < NB; j++) {
+                    const int pos = tid + T * (m0 + j);
+                    LineRef e = lr;
+                    set_pos(g, e, pos);
+                    op.post(lr.base + pos * g.estride, e, v[m0 + j], pre[j], acc);
+                }
+            }
         }
     }
     reduce_and_finalize<Op::NRED>(acc, rs, op);
@@ -309,7 +352,9 @@ k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__r
         LineRef lr = line_ref(g, blockIdx.x, line);
         if (lr.valid) {
             set_pos(g, lr, pos);
-            op.store(lr.base + pos * g.estride, lr, res[lay_idx(line, pos)], acc);
+            const long long ge = lr.base + pos * g.estride;
+            const typename Op::Pre pre = op.pre(ge);
+            op.post(ge, lr, res[lay_idx(line, pos)], pre, acc);
         }
     }
     reduce_and_finalize<Op::NRED>(acc, rs, op);

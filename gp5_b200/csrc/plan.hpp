@@ -55,6 +55,7 @@ struct gp5cu_plan {
     cudaStream_t own_stream = nullptr;
     gp5::AxisPlan ax[3];
     double *k2[3] = {nullptr, nullptr, nullptr};  // device k_d^2
+    double dk[3] = {0, 0, 0};                     // Fourier steps 2 pi / L_d
     std::vector<double> pos_host[3];              // cell-centred coordinates
     void *work = nullptr;                         // one field of FFT workspace
     double *partials = nullptr;
@@ -63,6 +64,7 @@ struct gp5cu_plan {
     gp5::DevScalars *ds = nullptr;
     unsigned long long *dmax = nullptr;
     int pw_blocks = 0;  // grid of the point-wise kernels
+    int sms = 148;      // multiprocessors of the device
     gp5::ProfRec *prof = nullptr;
 };
 
