@@ -39,10 +39,18 @@ C4 = 2.5
 SEED = 2024
 
 # algorithmic field transfers (read + write, units of one field) of each launch of an RK4
-# step, in launch order: per stage x-fwd, y-fwd, z (fwd * K^2 * inv), y-inv, x-inv
+# step, in launch order.  Merged path (16 launches): per stage y-fwd, z (fwd * K^2 * inv),
+# y-inv, x stage boundary (inverse x, stage epilogue, next stage prologue, forward x):
+#   boundary 1->2: R W, psi        W k1, W                         4
+#   boundary 2->3: R W, psi, k1    W k2, k1+2k2, W                 6
+#   boundary 3->4: R W, psi, k2, a W k3, a+2k3, W                  7
+#   boundary 4->1: R W, psi, k3, a W psi1, W                       6
+# Five-pass path (20 launches): per stage x-fwd, y-fwd, z, y-inv, x-inv.
+MERGED_BOUNDARY = [4, 6, 7, 6]
 STAGE_XFWD = [2, 3, 3, 3]
 STAGE_XINV = [3, 5, 6, 5]
-KIND_NAMES = {0: "x_fwd_prologue", 10: "y_fwd", 22: "z_fwd_kinetic_inv", 11: "y_inv", 1: "x_inv_epilogue"}
+KIND_NAMES = {0: "x_fwd_prologue", 10: "y_fwd", 22: "z_fwd_kinetic_inv", 11: "y_inv", 1: "x_inv_epilogue",
+              3: "x_stage_boundary"}
 
 
 def workload_geometry():
@@ -181,7 +189,7 @@ def run_ours(args, rank, world, local_rank):
                 torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
                 ms = float(t.item())
         lps = st.launches_per_step
-        launches += lps * args.steps
+        launches += lps * args.steps + 1  # + the prologue transform of each advance call
         r = {"ms": ms, "ms_per_step": ms / args.steps, "value": world * sites * args.steps / (ms / 1e3),
              "clocks": clk.summary(), "launches_per_step": lps}
         # per-launch durations of one step (CUDA events between launches, same stream)
@@ -208,7 +216,7 @@ def run_ours(args, rank, world, local_rank):
                     t = torch.tensor([ems], device=f"cuda:{dev}", dtype=torch.float64)
                     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
                     ems = float(t.item())
-            launches += lps * n_e2e
+            launches += (lps + 1) * n_e2e
             r["e2e"] = {"value": world * sites * n_e2e / (ems / 1e3), "unit": "site-updates/s",
                         "h2d_bytes_per_step": plan.field_bytes, "d2h_bytes_per_step": plan.field_bytes,
                         "steps": n_e2e, "ms_per_step": ems / n_e2e}
@@ -223,11 +231,15 @@ def roofline(r):
     """Dominant kernel (largest share of a step) with its algorithmic bytes per launch."""
     prof = r["profile"]
     F = r["field_bytes"]
-    if len(prof) != 20:
-        return None
     bytes_per = []
-    for s in range(4):
-        bytes_per += [STAGE_XFWD[s] * F, 2 * F, 2 * F, 2 * F, STAGE_XINV[s] * F]
+    if len(prof) == 16:
+        for s in range(4):
+            bytes_per += [2 * F, 2 * F, 2 * F, MERGED_BOUNDARY[s] * F]
+    elif len(prof) == 20:
+        for s in range(4):
+            bytes_per += [STAGE_XFWD[s] * F, 2 * F, 2 * F, 2 * F, STAGE_XINV[s] * F]
+    else:
+        return None
     tot = {}
     for (kind, ms), b in zip(prof, bytes_per):
         t = tot.setdefault(kind, [0.0, 0.0, 0])

@@ -30,7 +30,7 @@ void check_cuda(cudaError_t e, const char *what) {
 
 __global__ void k_set_scalars(DevScalars *ds) {
     ds->sigma[0] = ds->sigma[1] = 1.0;
-    ds->alpha[0] = ds->alpha[1] = 1.0;
+    ds->alpha[0][0] = ds->alpha[0][1] = ds->alpha[1][0] = ds->alpha[1][1] = 1.0;
     ds->status = 0u;
 }
 
@@ -656,10 +656,48 @@ int gp5cu_stepper_set_phase_constraint(gp5cu_stepper *st, const void *dphase) {
     GP5_CATCH
 }
 
-static int queue_step(gp5cu_stepper *st, void *field) {
+// The merged stage-boundary path runs when one component is stepped and the x axis uses the
+// register engine; otherwise each stage is five passes with separate prologue/epilogue.
+static bool merged_path(const gp5cu_plan *p) { return p->ncomp == 1 && p->ax[0].reg; }
+
+static int queue_step(gp5cu_stepper *st, void *field, bool merged, bool prologue) {
     int n = 0;
-    dispatch(st->func->plan, [&](auto r) { n = Launch<decltype(r)>::step(st, field); });
+    dispatch(st->func->plan, [&](auto r) {
+        n = merged ? Launch<decltype(r)>::step_merged(st, field, prologue) : Launch<decltype(r)>::step(st, field);
+    });
     return n;
+}
+
+// Captures one step into a CUDA graph bound to this field; kernels are configured in a dry
+// pass first so that no attribute call happens during the capture.
+static void build_graph(gp5cu_stepper *st, void *field, bool merged) {
+    gp5cu_plan *p = st->func->plan;
+    drop_graph(st);
+    p->dry = true;
+    try {
+        queue_step(st, field, merged, false);
+    } catch (...) {
+        p->dry = false;
+        throw;
+    }
+    p->dry = false;
+    cudaGraph_t g = nullptr;
+    check_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int n = 0;
+    try {
+        n = queue_step(st, field, merged, false);
+    } catch (...) {
+        cudaStreamEndCapture(p->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    check_cuda(cudaStreamEndCapture(p->stream, &g), "end capture");
+    cudaError_t e = cudaGraphInstantiate(&st->exec, g, 0);
+    cudaGraphDestroy(g);
+    check_cuda(e, "cudaGraphInstantiate");
+    st->graph_field = field;
+    st->graph_merged = merged;
+    st->launches_per_step = n;
 }
 
 int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
@@ -670,32 +708,15 @@ int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
     gp5cu_plan *p = st->func->plan;
     use_device(p);
     if (nsteps == 0) return GP5_OK;
+    const bool merged = merged_path(p);
+    if (!st->exec || st->graph_field != field || st->graph_merged != merged) build_graph(st, field, merged);
     set_scalars(p->stream, st->ds);
-    int done = 0;
-    if (!st->exec || st->graph_field != field) {
-        drop_graph(st);
-        // one eager step (sets kernel attributes), then capture a step into a graph
-        st->launches_per_step = queue_step(st, field);
-        st->t += st->dt;
-        done = 1;
-        if (nsteps > 1) {
-            cudaGraph_t g = nullptr;
-            check_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-            try {
-                queue_step(st, field);
-            } catch (...) {
-                cudaStreamEndCapture(p->stream, &g);
-                if (g) cudaGraphDestroy(g);
-                throw;
-            }
-            check_cuda(cudaStreamEndCapture(p->stream, &g), "end capture");
-            cudaError_t e = cudaGraphInstantiate(&st->exec, g, 0);
-            cudaGraphDestroy(g);
-            check_cuda(e, "cudaGraphInstantiate");
-            st->graph_field = field;
-        }
+    if (merged) {
+        // forward x transform of psi, consumed by the first graph step
+        p->dry = false;
+        dispatch(p, [&](auto r) { Launch<decltype(r)>::prologue(st, field); });
     }
-    for (int i = done; i < nsteps; i++) {
+    for (int i = 0; i < nsteps; i++) {
         check_cuda(cudaGraphLaunch(st->exec, p->stream), "cudaGraphLaunch");
         st->t += st->dt;
     }
@@ -754,12 +775,18 @@ int gp5cu_stepper_profile(gp5cu_stepper *st, void *field, int nrep, double *ms, 
     p->prof = &rec;
     try {
         set_scalars(p->stream, st->ds);
+        const bool merged = merged_path(p);
+        if (merged) {
+            p->prof = nullptr;
+            dispatch(p, [&](auto r) { Launch<decltype(r)>::prologue(st, field); });
+            p->prof = &rec;
+        }
         std::vector<double> acc;
         int n = 0;
         for (int r = 0; r < nrep; r++) {
             rec.idx = 0;
             rec.record(p->stream, -1);
-            n = queue_step(st, field);
+            n = queue_step(st, field, merged, false);
             st->t += st->dt;
             check_cuda(cudaStreamSynchronize(p->stream), "sync");
             if (acc.empty()) acc.assign(rec.idx - 1, 0.0);

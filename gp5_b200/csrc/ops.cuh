@@ -22,7 +22,7 @@ constexpr int kNRed = 8;
 // ---- device scalars shared by the kernels of one stepper / plan -------------------------
 struct DevScalars {
     double sigma[2];   // pending scale of the state (1 when clean)
-    double alpha[2];   // renormalisation factor of the current stage input
+    double alpha[2][2];  // [stage & 1][component]: scale of the stage's transform input
     double sums[8];    // last reduction result (raw sums, not yet times dV)
     double mu;         // chemical potential for the residual pass
     double factor;     // scale factor for normalize
@@ -92,6 +92,7 @@ template <typename Real, bool RED> struct OpStageIn {
     int use_sigma;
     Real cre, cim;
     double Nt0, Nt1, dV;
+    int slot;  // alpha slot (stage & 1) written by finalize
     __device__ __forceinline__ V load(long long g, const LineRef &e, double *acc) const {
         V p = psi[g];
         if (use_sigma) p = cscale(p, (Real)__ldg(&ds->sigma[e.c]));
@@ -119,9 +120,9 @@ template <typename Real, bool RED> struct OpStageIn {
     }
     __device__ __forceinline__ void finalize(const double *s) const {
         if (RED) {
-            ds->alpha[0] = sqrt(Nt0 / (dV * s[0]));
-            ds->alpha[1] = (Nt1 > 0) ? sqrt(Nt1 / (dV * s[1])) : 1.0;
-            if (!isfinite(s[0]) || !isfinite(s[1]) || !isfinite(ds->alpha[0])) ds->status |= DS_NONFINITE;
+            ds->alpha[slot][0] = sqrt(Nt0 / (dV * s[0]));
+            ds->alpha[slot][1] = (Nt1 > 0) ? sqrt(Nt1 / (dV * s[1])) : 1.0;
+            if (!isfinite(s[0]) || !isfinite(s[1]) || !isfinite(ds->alpha[slot][0])) ds->status |= DS_NONFINITE;
         }
     }
 };
@@ -151,8 +152,13 @@ template <typename Real> struct EpiParams {
     const V *tsrc; // kinetic buffer for the non-fused (2 component) epilogue
     DevScalars *ds;
     int use_sigma, use_alpha;
+    int slot;       // alpha slot of this stage (stage & 1)
+    int u1_raw;     // first stage / Euler: the transform input was the raw state (its pending
+                    // scale sigma is folded into alpha by the previous step)
     Real cre, cim;  // stage coefficient of u~ = sigma psi - c kprev
     Real dre, dim;  // tau (Euler) or tau/6 (RK4)
+    int turn;       // also form the next stage's transform input (stage boundary kernel)
+    Real cnre, cnim;  // next stage: u~' = sigma psi - cn k_s (RK1..RK3); psi1 for RK4/Euler
     // functional
     int fkind;
     int has_g;
@@ -257,20 +263,24 @@ __device__ __forceinline__ EpiIn<Real> epi_load(const EpiParams<Real> &P, long l
     return in;
 }
 
+// With P.turn the epilogue also returns, in next[c], the input of the following transform:
+// u~_{s+1} = sigma psi - cn k_s after stages 1-3, or the new state psi1 after the last stage
+// (and Euler); with RED it accumulates |next|^2 for the following normalisation.
 template <typename Real, int NC, bool RED>
 __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long long s, int i, int j, int k,
                                               const cpx<Real> (&t)[NC], const EpiIn<Real> (&in)[NC],
-                                              double *acc) {
+                                              double *acc, cpx<Real> (&next)[NC]) {
     using V = cpx<Real>;
     V p[NC], u[NC], kin[NC], h[NC];
     Real Vv[NC], nn[NC];
     const int mode = P.mode;
 #pragma unroll
     for (int c = 0; c < NC; c++) {
-        V x = in[c].psi;
+        const V raw = in[c].psi;
+        V x = raw;
         if (P.use_sigma) x = cscale(x, (Real)__ldg(&P.ds->sigma[c]));
         p[c] = x;
-        V ut = x;
+        V ut = P.u1_raw ? raw : x;
         if (mode >= EPI_RK2) {
             V c0;
             c0.x = P.cre;
@@ -278,7 +288,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long lon
             ut = csub(x, cmul(c0, in[c].kprev));
         }
         if (P.use_alpha) {
-            const Real a = (Real)__ldg(&P.ds->alpha[c]);
+            const Real a = (Real)__ldg(&P.ds->alpha[P.slot][c]);
             u[c] = cscale(ut, a);
             kin[c] = cscale(t[c], a);
         } else {
@@ -304,26 +314,27 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long lon
         }
         return;
     }
-    if (mode == EPI_RK1) {
-#pragma unroll
-        for (int c = 0; c < NC; c++) P.kout[s + (long long)c * P.nsites] = h[c];
-        return;
-    }
-    if (mode == EPI_RK2) {
+    if (mode == EPI_RK1 || mode == EPI_RK2 || mode == EPI_RK3) {
 #pragma unroll
         for (int c = 0; c < NC; c++) {
             const long long g = s + (long long)c * P.nsites;
-            P.kout[g] = h[c];
-            P.kacc[g] = cadd(in[c].kprev, cscale(h[c], (Real)2));
-        }
-        return;
-    }
-    if (mode == EPI_RK3) {
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-            const long long g = s + (long long)c * P.nsites;
-            P.kacc[g] = cadd(in[c].kacc, cscale(h[c], (Real)2));
-            P.kout[g] = h[c];
+            if (mode == EPI_RK1) {
+                P.kout[g] = h[c];
+            } else if (mode == EPI_RK2) {
+                P.kout[g] = h[c];
+                P.kacc[g] = cadd(in[c].kprev, cscale(h[c], (Real)2));
+            } else {
+                P.kacc[g] = cadd(in[c].kacc, cscale(h[c], (Real)2));
+                P.kout[g] = h[c];
+            }
+            if (P.turn) {
+                V cn;
+                cn.x = P.cnre;
+                cn.y = P.cnim;
+                const V nx = csub(p[c], cmul(cn, h[c]));
+                next[c] = nx;
+                if (RED) acc[c] += (double)nx.x * (double)nx.x + (double)nx.y * (double)nx.y;
+            }
         }
         return;
     }
@@ -342,6 +353,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, long lon
             r = cscale(P.phase_exp[g], a);
         }
         P.psi_out[g] = r;
+        if (P.turn) next[c] = r;
         if (RED && P.renorm_out) acc[c] += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
     }
 }
@@ -357,25 +369,50 @@ template <typename Real> struct EpiFinalize {
         } else if ((P.mode == EPI_EULER || P.mode == EPI_RK4) && P.renorm_out) {
             ds->sigma[0] = sqrt(P.Nt0 / (P.dV * s[0]));
             ds->sigma[1] = (P.Nt1 > 0) ? sqrt(P.Nt1 / (P.dV * s[1])) : 1.0;
+            if (P.turn) {
+                // the next step transforms the raw state: its first stage scales by sigma
+                ds->alpha[1][0] = ds->sigma[0];
+                ds->alpha[1][1] = ds->sigma[1];
+            }
             if (!isfinite(s[0]) || !isfinite(ds->sigma[0])) ds->status |= DS_NONFINITE;
+        } else if (P.turn && P.renorm_out) {
+            // normalisation of the next stage's input u~_{s+1} (slot of stage s+1)
+            const int ns = P.slot ^ 1;
+            ds->alpha[ns][0] = sqrt(P.Nt0 / (P.dV * s[0]));
+            ds->alpha[ns][1] = (P.Nt1 > 0) ? sqrt(P.Nt1 / (P.dV * s[1])) : 1.0;
+            if (!isfinite(s[0]) || !isfinite(ds->alpha[ns][0])) ds->status |= DS_NONFINITE;
         }
     }
 };
 
 // Fused epilogue (one component): the inverse x pass hands every element to the site logic.
-template <typename Real, bool RED> struct OpStageOut {
+// TURN (stage boundary, mode inverse -> turn -> forward): turn() runs the epilogue of stage s
+// and returns the next stage's transform input; post() stores the forward transform into src.
+template <typename Real, bool RED, bool TURN = false> struct OpStageOut {
     static constexpr int NRED = RED ? kNRed : 0, BATCH = 2;
     using V = cpx<Real>;
     using Pre = EpiIn<Real>;
-    const V *src;  // inverse-pass input buffer
+    const V *src;  // inverse-pass input buffer (the boundary kernel writes it back in place)
     EpiParams<Real> P;
     __device__ __forceinline__ V load(long long g, const LineRef &, double *) const { return src[g]; }
     __device__ __forceinline__ V mid(V v, const LineRef &) const { return v; }
     __device__ __forceinline__ Pre pre(long long g) const { return epi_load(P, g); }
-    __device__ __forceinline__ void post(long long g, const LineRef &e, V v, const Pre &in, double *acc) const {
+    __device__ __forceinline__ V turn(long long g, const LineRef &e, V v, const Pre &in, double *acc) const {
         const V t[1] = {v};
         const Pre ins[1] = {in};
-        epilogue_site<Real, 1, RED>(P, g, e.i, e.j, e.k, t, ins, acc);
+        V nx[1] = {v};
+        epilogue_site<Real, 1, RED>(P, g, e.i, e.j, e.k, t, ins, acc, nx);
+        return nx[0];
+    }
+    __device__ __forceinline__ void post(long long g, const LineRef &e, V v, const Pre &in, double *acc) const {
+        if (TURN) {
+            const_cast<V *>(src)[g] = v;
+        } else {
+            const V t[1] = {v};
+            const Pre ins[1] = {in};
+            V nx[1];
+            epilogue_site<Real, 1, RED>(P, g, e.i, e.j, e.k, t, ins, acc, nx);
+        }
     }
     __device__ __forceinline__ int streams(const void *(&p)[4]) const {
         int n = 0;
@@ -404,7 +441,8 @@ template <typename Real, int NC, bool RED> struct OpSiteEpilogue {
         const int i = (int)(s % P.nx);
         const long long r = s / P.nx;
         const int j = (int)(r % P.ny), k = (int)(r / P.ny);
-        epilogue_site<Real, NC, RED>(P, s, i, j, k, t, in, acc);
+        V nx[NC];
+        epilogue_site<Real, NC, RED>(P, s, i, j, k, t, in, acc, nx);
     }
     __device__ __forceinline__ void finalize(const double *s) const { EpiFinalize<Real>::run(P, s); }
 };

@@ -19,7 +19,9 @@
 
 namespace gp5 {
 
-enum PassMode : int { MODE_FWD = 0, MODE_INV = 1, MODE_FWD_MID_INV = 2 };
+// MODE_INV_TURN_FWD: inverse transform, op.turn() per element (epilogue of one stage and
+// prologue of the next), forward transform, op.post() stores.
+enum PassMode : int { MODE_FWD = 0, MODE_INV = 1, MODE_FWD_MID_INV = 2, MODE_INV_TURN_FWD = 3 };
 
 struct TileGeom {
     int nx, ny, nz, nc;
@@ -169,9 +171,9 @@ __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// L2 prefetch of the auxiliary streams (every stream but the first, which the prologue loads
-// at once) of a contiguous x tile: one instruction per stream, issued by thread 0 at kernel
-// start, so that the epilogue's operand loads hit L2 while the transform runs.
+// L2 prefetch of every stream of a contiguous x tile that reads more than one array: one
+// instruction per stream, issued by thread 0 at kernel start, so that all DRAM reads of the
+// tile are in flight at once and the later register loads hit L2.
 template <typename V, class Op>
 __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, const Op &op) {
     const void *st[4];
@@ -181,25 +183,33 @@ __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, 
     long long L1 = L0 + g.lines;
     if (L1 > g.n_other) L1 = g.n_other;
     const long long e0 = L0 * g.nx, cnt = (L1 - L0) * g.nx;
-    for (int q = 1; q < ns; q++)
+    for (int q = 0; q < ns; q++)
         prefetch_l2(reinterpret_cast<const V *>(st[q]) + e0, (unsigned)(cnt * sizeof(V)));
 }
 
 // ---- register-engine kernel ----------------------------------------------------------------
-// Threads: LINES lines x T threads per line; 256 threads for every supported N; one tile per
+// Threads: LINES lines x T threads per line (RegTile below); one tile per
 // CTA.
-template <int N> struct RegTile {
+// Tile shape: the passes with two transforms (forward*K^2*inverse, and the stage boundary)
+// have the longest compute phase; they use 128-thread tiles so that several small CTAs share
+// an SM and their load / transform / store phases interleave.  Copy passes use 256 threads.
+#ifndef GP5_HEAVY_THREADS
+#define GP5_HEAVY_THREADS 128
+#endif
+template <typename Real, int N, bool CONTIG, int MODE> struct RegTile {
     static constexpr int T = RegCfgAll<N>::T;
-    static constexpr int LINES = 256 / T;
+    static constexpr int THREADS =
+        (MODE == MODE_FWD_MID_INV || MODE == MODE_INV_TURN_FWD) && GP5_HEAVY_THREADS / T >= 2 ? GP5_HEAVY_THREADS : 256;
+    static constexpr int LINES = THREADS / T;
+    // register cap: 128 per thread for complex128, 80 for complex64
+    static constexpr int MINB = (sizeof(Real) == 8 ? 65536 / 128 : 65536 / 80) / THREADS;
 };
 
-template <typename Real> struct RegOcc { static constexpr int value = sizeof(Real) == 8 ? 2 : 3; };
-
 template <typename Real, int N, bool CONTIG, int MODE, class Op>
-__global__ void __launch_bounds__(256, RegOcc<Real>::value)
+__global__ void __launch_bounds__(RegTile<Real, N, CONTIG, MODE>::THREADS, RegTile<Real, N, CONTIG, MODE>::MINB)
 k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedSlot rs) {
     using V = cpx<Real>;
-    constexpr int E = RegCfg<N>::E, T = RegCfgAll<N>::T, LINES = RegTile<N>::LINES;
+    constexpr int E = RegCfg<N>::E, T = RegCfgAll<N>::T, LINES = RegTile<Real, N, CONTIG, MODE>::LINES;
     constexpr int NB = Op::BATCH;
     static_assert(E % NB == 0, "batch must divide the elements per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -229,7 +239,27 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 v[m] = mk<Real>(0, 0);
             }
         }
-        if constexpr (CONTIG) {
+        if constexpr (MODE == MODE_INV_TURN_FWD) {
+            static_assert(CONTIG, "the stage boundary runs on x lines");
+            LayContig<N> lay;
+            reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += NB) {
+                typename Op::Pre pre[NB];
+#pragma unroll
+                for (int j = 0; j < NB; j++)
+                    pre[j] = lr.valid ? op.pre(lr.base + (tid + T * (m0 + j)) * g.estride) : typename Op::Pre{};
+#pragma unroll
+                for (int j = 0; j < NB; j++) {
+                    const int pos = tid + T * (m0 + j);
+                    LineRef e = lr;
+                    set_pos(g, e, pos);
+                    if (lr.valid) v[m0 + j] = op.turn(lr.base + pos * g.estride, e, v[m0 + j], pre[j], acc);
+                }
+            }
+            __syncthreads();
+            reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+        } else if constexpr (CONTIG) {
             LayContig<N> lay;
             if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
             else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
@@ -258,7 +288,15 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 reg_fft<N, 1>(v, tid, line, tw, sm, lay);
             }
         }
-        if (lr.valid) {
+        if (lr.valid && MODE == MODE_INV_TURN_FWD) {
+#pragma unroll
+            for (int m = 0; m < E; m++) {
+                const int pos = tid + T * m;
+                LineRef e = lr;
+                set_pos(g, e, pos);
+                op.post(lr.base + pos * g.estride, e, v[m], typename Op::Pre{}, acc);
+            }
+        } else if (lr.valid) {
             // epilogue in batches: the operand loads of NB elements are issued together
 #pragma unroll
             for (int m0 = 0; m0 < E; m0 += NB) {

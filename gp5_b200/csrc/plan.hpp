@@ -66,6 +66,7 @@ struct gp5cu_plan {
     int pw_blocks = 0;  // grid of the point-wise kernels
     int sms = 148;      // multiprocessors of the device
     gp5::ProfRec *prof = nullptr;
+    bool dry = false;  // launch helpers only configure kernels (before a stream capture)
 };
 
 struct gp5cu_functional {
@@ -89,8 +90,7 @@ struct gp5cu_stepper {
     gp5::DevScalars *ds = nullptr;
     cudaGraphExec_t exec = nullptr;
     void *graph_field = nullptr;
-    bool graph_renorm = false;
-    const void *graph_phase = nullptr;
+    bool graph_merged = false;
     double t = 0;
     int launches_per_step = 0;
 };
@@ -108,6 +108,8 @@ template <typename Real> struct Launch {
     static void max_density(gp5cu_plan *p, const void *field);
     static void convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128);
     static int step(gp5cu_stepper *st, void *field);  // queue one step; returns launches
+    static int step_merged(gp5cu_stepper *st, void *field, bool prologue);
+    static void prologue(gp5cu_stepper *st, void *field);  // forward x transform of psi
     static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
 };
 
