@@ -111,6 +111,7 @@ def lib():
         "gp5cu_stepper_advance_host": (i, [vp, vp, vp, i]),
         "gp5cu_stepper_launches_per_step": (i, [vp]),
         "gp5cu_stepper_profile": (i, [vp, vp, i, C.POINTER(d), C.POINTER(i), i, C.POINTER(i)]),
+        "gp5cu_norm_noalloc": (i, [vp, i, C.POINTER(C.c_int), i, i, d, vp, C.POINTER(d)]),
     }
     for name, (res, args) in proto.items():
         f = getattr(L, name)

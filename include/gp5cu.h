@@ -178,6 +178,22 @@ int gp5cu_stepper_launches_per_step(const gp5cu_stepper *st);
 int gp5cu_stepper_profile(gp5cu_stepper *st, void *dfield, int nrep, double *ms, int *kinds, int cap,
                           int *nlaunch);
 
+/* ---- allocation-free norm ---------------------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc when they need
+ * a norm (their device memory belongs to another allocator, or the device is full): the same
+ * value as gp5cu_norm, dV * sum |psi_comp|^2, computed without a plan and without allocating.
+ * Its scratch (block partial sums, a ticket, the result slot) is a file-scope static device
+ * array of 33,024 bytes that every GPU loading the library keeps until the process exits.
+ * Limit: at most GP5_NOALLOC_MAX_SITES sites (256^3); larger fields return GP5_ERR_ARG.
+ * dfield: device field (shape[0]*shape[1]*shape[2] sites, ncomp components, `precision`) on
+ * the current device; stream: cudaStream_t or NULL; *out receives the norm (host), after
+ * the stream is synchronised.  The first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress): make it before any stream capture.  Calls share the scratch, so
+ * calls that overlap on the GPU race. */
+#define GP5_NOALLOC_MAX_SITES 16777216LL
+int gp5cu_norm_noalloc(const void *dfield, int precision, const int shape[3], int ncomp, int comp,
+                       double dV, void *stream, double *out);
+
 #ifdef __cplusplus
 }
 #endif
