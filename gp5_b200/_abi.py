@@ -58,6 +58,19 @@ class Observables(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class SolveDesc(C.Structure):
+    _fields_ = [("n", C.c_int), ("L", C.c_double), ("N", C.c_double), ("c3", C.c_double), ("c4", C.c_double),
+                ("omega", C.c_double), ("dt", C.c_double)]
+
+
+class SolveResult(C.Structure):
+    _fields_ = [("steps", C.c_int), ("converged", C.c_int), ("residual", C.c_double), ("energy", C.c_double),
+                ("mu", C.c_double), ("norm", C.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 def header_functions(path: str = HEADER):
     """Names of every function declared in include/gp5cu.h."""
     txt = open(path).read()
@@ -112,6 +125,12 @@ def lib():
         "gp5cu_stepper_launches_per_step": (i, [vp]),
         "gp5cu_stepper_profile": (i, [vp, vp, i, C.POINTER(d), C.POINTER(i), i, C.POINTER(i)]),
         "gp5cu_norm_noalloc": (i, [vp, i, C.POINTER(C.c_int), i, i, d, vp, C.POINTER(d)]),
+        "gp5cu_batch_create": (i, [pp, i, C.POINTER(SolveDesc), i, i]),
+        "gp5cu_batch_destroy": (i, [vp]),
+        "gp5cu_batch_set_state": (i, [vp, i, vp]),
+        "gp5cu_batch_get_state": (i, [vp, i, vp]),
+        "gp5cu_batch_solve": (i, [vp, d, i, i, C.POINTER(SolveResult)]),
+        "gp5cu_batch_launches": (C.c_longlong, [vp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(L, name)
@@ -357,6 +376,53 @@ class Stepper:
         if getattr(self, "h", None) and getattr(self.func.plan, "h", None):
             lib().gp5cu_stepper_destroy(self.h)
         self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent LHY droplet ground-state solves advanced together (gp5cu_batch_*).
+
+    solves: list of dicts with n, L, N, c3, c4, omega, dt.
+    """
+
+    def __init__(self, solves, precision: int = GP5_C128, device: int = 0):
+        arr = (SolveDesc * len(solves))()
+        for k, sd in enumerate(solves):
+            arr[k] = SolveDesc(int(sd["n"]), float(sd["L"]), float(sd["N"]), float(sd.get("c3", -3.0)),
+                               float(sd.get("c4", 2.5)), float(sd.get("omega", 0.0)), float(sd["dt"]))
+        self.solves = [dict(sd) for sd in solves]
+        h = C.c_void_p()
+        check(lib().gp5cu_batch_create(C.byref(h), len(solves), arr, precision, device))
+        self.h = h
+
+    def set_state(self, k: int, psi: np.ndarray) -> None:
+        a = np.asfortranarray(np.asarray(psi, dtype=np.complex128).reshape((self.solves[k]["n"],) * 3, order="F"))
+        check(lib().gp5cu_batch_set_state(self.h, k, C.c_void_p(_ptr(a))))
+
+    def get_state(self, k: int) -> np.ndarray:
+        n = self.solves[k]["n"]
+        out = np.empty((n, n, n, 1), dtype=np.complex128, order="F")
+        check(lib().gp5cu_batch_get_state(self.h, k, C.c_void_p(_ptr(out))))
+        return out
+
+    def solve(self, tol: float, check_every: int = 100, max_steps: int = 100000):
+        res = (SolveResult * len(self.solves))()
+        check(lib().gp5cu_batch_solve(self.h, float(tol), int(check_every), int(max_steps), res))
+        return [r.as_dict() for r in res]
+
+    @property
+    def launches(self) -> int:
+        return int(lib().gp5cu_batch_launches(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gp5cu_batch_destroy(self.h)
+            self.h = None
 
     def __del__(self):
         try:

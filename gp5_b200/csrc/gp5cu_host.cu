@@ -28,10 +28,12 @@ void check_cuda(cudaError_t e, const char *what) {
     }
 }
 
-__global__ void k_set_scalars(DevScalars *ds) {
-    ds->sigma[0] = ds->sigma[1] = 1.0;
-    ds->alpha[0][0] = ds->alpha[0][1] = ds->alpha[1][0] = ds->alpha[1][1] = 1.0;
-    ds->status = 0u;
+__global__ void k_set_scalars(DevScalars *ds, int n) {
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        ds[q].sigma[0] = ds[q].sigma[1] = 1.0;
+        ds[q].alpha[0][0] = ds[q].alpha[0][1] = ds[q].alpha[1][0] = ds[q].alpha[1][1] = 1.0;
+        ds[q].status = 0u;
+    }
 }
 
 void smem_opt_in(const void *kernel, size_t bytes, int dev) {
@@ -71,8 +73,8 @@ void ProfRec::record(cudaStream_t s, int kind) {
     idx++;
 }
 
-void set_scalars(cudaStream_t s, DevScalars *ds) {
-    k_set_scalars<<<1, 1, 0, s>>>(ds);
+void set_scalars(cudaStream_t s, DevScalars *ds, int n) {
+    k_set_scalars<<<1, 128, 0, s>>>(ds, n);
     check_cuda(cudaGetLastError(), "k_set_scalars");
 }
 
@@ -175,6 +177,95 @@ template <class F> static void dispatch(const gp5cu_plan *p, F &&f) {
     else f((float)0);
 }
 
+// Geometry of one solve (gp::discretization for one rank, src/geometry.h:88-90): Fourier
+// steps 2 pi / L, cell-centred positions, dV as the product of the space steps in axis order
+// (src/geometry.cpp:206-210); the kinetic factor is that of the Laplacian (-1/N^3).
+static SolveParams geometry_params(const int shape[3], const double left[3], const double right[3]) {
+    SolveParams S{};
+    double dv = 1.0;
+    long long n = 1;
+    for (int d = 0; d < 3; d++) {
+        const double L = right[d] - left[d];
+        S.dk[d] = 2 * M_PI / L;
+        S.left[d] = left[d];
+        S.dx[d] = L / shape[d];
+        dv *= S.dx[d];
+        n *= shape[d];
+    }
+    S.dV = dv;
+    S.kin[0] = S.kin[1] = -1.0 / (double)n;
+    S.active = 1;
+    return S;
+}
+
+// A plan for nsolve independent solves of one grid (boxes may differ per solve).
+gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const double *const *rights, int nsolve,
+                        int ncomp, int precision, int device) {
+    require(ncomp == 1 || ncomp == 2, "ncomp must be 1 or 2");
+    require(precision == GP5_C128 || precision == GP5_C64, "precision must be GP5_C128 or GP5_C64");
+    require(nsolve >= 1 && nsolve <= 4096, "between 1 and 4096 solves per plan");
+    for (int d = 0; d < 3; d++) require(shape[d] >= 2 && shape[d] <= 4096, "each axis length must be in [2, 4096]");
+    for (int q = 0; q < nsolve; q++)
+        for (int d = 0; d < 3; d++) require(rights[q][d] > lefts[q][d], "domain right must exceed left on every axis");
+    int ndev = 0;
+    check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    require(device >= 0 && device < ndev, "device ordinal out of range");
+    gp5cu_plan *p = new gp5cu_plan();
+    try {
+        p->dev = device;
+        check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        for (int d = 0; d < 3; d++) {
+            p->shape[d] = shape[d];
+            p->left[d] = lefts[0][d];
+            p->right[d] = rights[0][d];
+        }
+        p->ncomp = ncomp;
+        p->prec = precision;
+        p->nsites = (long long)shape[0] * shape[1] * shape[2];
+        p->nsolve = nsolve;
+        p->solve_stride = p->nsites * ncomp;
+        p->elem_bytes = precision == GP5_C128 ? 16 : 8;
+        p->field_bytes = (size_t)p->nsites * ncomp * p->elem_bytes;
+        p->sp_host.resize(nsolve);
+        for (int q = 0; q < nsolve; q++) p->sp_host[q] = geometry_params(shape, lefts[q], rights[q]);
+        p->dV = p->sp_host[0].dV;
+        check_cuda(cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        p->stream = p->own_stream;
+        for (int d = 0; d < 3; d++) build_axis_plan(p, d);
+        check_cuda(cudaMalloc(&p->work, p->field_bytes * nsolve), "cudaMalloc work");
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        p->sms = sms;
+        p->pw_blocks = sms * 8;
+        p->pw_bps = std::max(1, p->pw_blocks / nsolve);
+        // partial-sum slots per solve: the most blocks any kernel gives one solve (at worst one
+        // line per tile)
+        long long mb = p->pw_bps;
+        for (int d = 0; d < 3; d++) {
+            const long long lines_total = d == 0 ? (long long)shape[1] * shape[2] * ncomp
+                                                 : (d == 1 ? (long long)shape[0] * shape[2] * ncomp
+                                                           : (long long)shape[0] * shape[1] * ncomp);
+            mb = std::max(mb, lines_total);
+        }
+        p->max_blocks = mb;
+        check_cuda(cudaMalloc(&p->partials, sizeof(double) * kNRed * mb * nsolve), "cudaMalloc partials");
+        check_cuda(cudaMalloc(&p->counter, sizeof(unsigned) * nsolve), "cudaMalloc counter");
+        check_cuda(cudaMemset(p->counter, 0, sizeof(unsigned) * nsolve), "memset counter");
+        check_cuda(cudaMalloc(&p->ds, sizeof(DevScalars) * nsolve), "cudaMalloc scalars");
+        check_cuda(cudaMemset(p->ds, 0, sizeof(DevScalars) * nsolve), "memset scalars");
+        check_cuda(cudaMalloc(&p->sp_lap, sizeof(SolveParams) * nsolve), "cudaMalloc params");
+        check_cuda(cudaMemcpy(p->sp_lap, p->sp_host.data(), sizeof(SolveParams) * nsolve, cudaMemcpyHostToDevice),
+                   "upload params");
+        check_cuda(cudaMalloc(&p->dmax, sizeof(unsigned long long)), "cudaMalloc dmax");
+        set_scalars(p->stream, p->ds, nsolve);
+        check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    } catch (...) {
+        gp5cu_plan_destroy(p);
+        throw;
+    }
+    return p;
+}
+
 extern "C" {
 
 int gp5cu_version(void) { return 10000; }
@@ -201,86 +292,7 @@ int gp5cu_plan_create(gp5cu_plan **out, const int shape[3], const double left[3]
     require(out != nullptr, "out is NULL");
     *out = nullptr;
     require(shape && left && right, "shape/left/right must not be NULL");
-    require(ncomp == 1 || ncomp == 2, "ncomp must be 1 or 2");
-    require(precision == GP5_C128 || precision == GP5_C64, "precision must be GP5_C128 or GP5_C64");
-    for (int d = 0; d < 3; d++) {
-        require(shape[d] >= 2 && shape[d] <= 4096, "each axis length must be in [2, 4096]");
-        require(right[d] > left[d], "domain right must exceed left on every axis");
-    }
-    int ndev = 0;
-    check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
-    require(device >= 0 && device < ndev, "device ordinal out of range");
-    gp5cu_plan *p = new gp5cu_plan();
-    try {
-        p->dev = device;
-        use_device(p);
-        for (int d = 0; d < 3; d++) {
-            p->shape[d] = shape[d];
-            p->left[d] = left[d];
-            p->right[d] = right[d];
-        }
-        p->ncomp = ncomp;
-        p->prec = precision;
-        p->nsites = (long long)shape[0] * shape[1] * shape[2];
-        p->elem_bytes = precision == GP5_C128 ? 16 : 8;
-        p->field_bytes = (size_t)p->nsites * ncomp * p->elem_bytes;
-        // dV = product of space steps in axis order (geometry.cpp:206-210)
-        double dv = 1.0;
-        for (int d = 0; d < 3; d++) dv *= (right[d] - left[d]) / shape[d];
-        p->dV = dv;
-        check_cuda(cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        p->stream = p->own_stream;
-        for (int d = 0; d < 3; d++) {
-            build_axis_plan(p, d);
-            // k_d = (2 pi / L) m, m = i (i < n/2, even n; i <= (n-1)/2, odd n) else i - n
-            // (geometry.cpp:108-152); tabulated squared, as K*K in operators.cpp:20.
-            const int n = shape[d];
-            const double delta = 2 * M_PI / (right[d] - left[d]);
-            p->dk[d] = delta;
-            std::vector<double> k2(n);
-            p->pos_host[d].resize(n);
-            const double dx = (right[d] - left[d]) / n;
-            for (int i = 0; i < n; i++) {
-                double k;
-                if (n % 2 == 0) k = (i < n / 2) ? delta * i : (-n + i) * delta;
-                else k = (i <= (n - 1) / 2) ? delta * i : (-n + i) * delta;
-                k2[i] = k * k;
-                p->pos_host[d][i] = left[d] + dx * (i + 0.5);  // geometry.cpp:184
-            }
-            check_cuda(cudaMalloc(&p->k2[d], sizeof(double) * n), "cudaMalloc k2");
-            check_cuda(cudaMemcpy(p->k2[d], k2.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload k2");
-        }
-        check_cuda(cudaMalloc(&p->work, p->field_bytes), "cudaMalloc work");
-        // partial-sum slots: the largest grid any kernel of this plan launches
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        p->sms = sms;
-        p->pw_blocks = sms * 8;
-        long long mb = p->pw_blocks;
-        for (int d = 0; d < 3; d++) {
-            const int lines_reg = 256 / (p->shape[d] <= 64 ? 8 : (p->shape[d] == 512 ? 64 : 16));
-            const int lines = std::min(lines_reg, p->ax[d].smem_lines);
-            // worst case: one line per tile
-            long long lines_total = d == 0 ? (long long)shape[1] * shape[2] * ncomp
-                                           : (d == 1 ? (long long)shape[0] * shape[2] * ncomp
-                                                     : (long long)shape[0] * shape[1] * ncomp);
-            (void)lines;
-            mb = std::max(mb, lines_total);
-        }
-        p->max_blocks = mb;
-        check_cuda(cudaMalloc(&p->partials, sizeof(double) * kNRed * mb), "cudaMalloc partials");
-        check_cuda(cudaMalloc(&p->counter, sizeof(unsigned)), "cudaMalloc counter");
-        check_cuda(cudaMemset(p->counter, 0, sizeof(unsigned)), "memset counter");
-        check_cuda(cudaMalloc(&p->ds, sizeof(DevScalars)), "cudaMalloc scalars");
-        check_cuda(cudaMemset(p->ds, 0, sizeof(DevScalars)), "memset scalars");
-        check_cuda(cudaMalloc(&p->dmax, sizeof(unsigned long long)), "cudaMalloc dmax");
-        set_scalars(p->stream, p->ds);
-        check_cuda(cudaStreamSynchronize(p->stream), "sync");
-    } catch (...) {
-        gp5cu_plan_destroy(p);
-        throw;
-    }
-    *out = p;
+    *out = create_plan(shape, &left, &right, 1, ncomp, precision, device);
     GP5_CATCH
 }
 
@@ -288,10 +300,8 @@ int gp5cu_plan_destroy(gp5cu_plan *p) {
     if (!p) return GP5_OK;
     cudaSetDevice(p->dev);
     if (p->stream) cudaStreamSynchronize(p->stream);
-    for (int d = 0; d < 3; d++) {
-        cudaFree(p->ax[d].tw);
-        cudaFree(p->k2[d]);
-    }
+    for (int d = 0; d < 3; d++) cudaFree(p->ax[d].tw);
+    cudaFree(p->sp_lap);
     cudaFree(p->work);
     cudaFree(p->partials);
     cudaFree(p->counter);
@@ -371,7 +381,7 @@ int gp5cu_upload_c128(gp5cu_plan *p, void *dfield, const double *host) {
     check_cuda(cudaMalloc(&tmp, n * 16), "cudaMalloc staging");
     try {
         check_cuda(cudaMemcpyAsync(tmp, host, n * 16, cudaMemcpyHostToDevice, p->stream), "upload");
-        Launch<float>::convert(p, tmp, dfield, nullptr, nullptr);
+        Launch<float>::convert(p, tmp, dfield, nullptr, nullptr, (long long)n);
         check_cuda(cudaStreamSynchronize(p->stream), "sync");
     } catch (...) {
         cudaFree(tmp);
@@ -391,7 +401,7 @@ int gp5cu_download_c128(gp5cu_plan *p, const void *dfield, double *host) {
     double *tmp = nullptr;
     check_cuda(cudaMalloc(&tmp, n * 16), "cudaMalloc staging");
     try {
-        Launch<float>::convert(p, nullptr, nullptr, dfield, tmp);
+        Launch<float>::convert(p, nullptr, nullptr, dfield, tmp, (long long)n);
         check_cuda(cudaMemcpyAsync(host, tmp, n * 16, cudaMemcpyDeviceToHost, p->stream), "download");
         check_cuda(cudaStreamSynchronize(p->stream), "sync");
     } catch (...) {
@@ -476,6 +486,36 @@ void gp5cu_functional_desc_init(gp5cu_functional_desc *d) {
     d->potential = GP5_POT_NONE;
 }
 
+// Parameters of the functional on top of the plan's geometry, for every solve of the plan.
+extern "C++" {
+void fill_functional_params(const gp5cu_plan *p, const gp5cu_functional_desc &d, SolveParams &S) {
+    for (int c = 0; c < 2; c++) {
+        const double m = (d.kind == GP5_FUNC_GP && c < p->ncomp) ? d.masses[c] : 1.0;
+        require(m > 0, "masses must be positive");
+        // -1/2 (1/m) IFFT(-K^2 FFT)/N^3 = IFFT(K^2 FFT) * (0.5/m/N^3)
+        S.kin[c] = 0.5 * (1.0 / m) / (double)p->nsites;
+    }
+    S.c3 = d.c3;
+    S.c4 = d.c4;
+    S.g00 = d.couplings[0];
+    S.g01 = d.couplings[1];
+    S.g11 = d.couplings[3];
+    S.la = d.alpha;
+    S.lb = d.beta;
+    S.le = d.eta;
+    for (int c = 0; c < 2; c++)
+        for (int k = 0; k < 3; k++)  // w*w as in externalPotential.cpp:26
+            S.om2[c][k] = (d.potential == GP5_POT_HARMONIC && c < p->ncomp) ? d.omegas[c][k] * d.omegas[c][k] : 0.0;
+}
+}  // extern "C++"
+
+extern "C++" {
+void upload_params(const std::vector<SolveParams> &h, SolveParams **dptr) {
+    if (!*dptr) check_cuda(cudaMalloc(dptr, sizeof(SolveParams) * h.size()), "cudaMalloc params");
+    check_cuda(cudaMemcpy(*dptr, h.data(), sizeof(SolveParams) * h.size(), cudaMemcpyHostToDevice), "upload params");
+}
+}  // extern "C++"
+
 int gp5cu_functional_create(gp5cu_plan *p, const gp5cu_functional_desc *desc, gp5cu_functional **out) {
     GP5_TRY
     require(p && desc && out, "NULL argument");
@@ -490,28 +530,9 @@ int gp5cu_functional_create(gp5cu_plan *p, const gp5cu_functional_desc *desc, gp
     f->plan = p;
     f->desc = *desc;
     try {
-        for (int c = 0; c < p->ncomp; c++) {
-            const double m = (desc->kind == GP5_FUNC_GP) ? desc->masses[c] : 1.0;
-            require(m > 0, "masses must be positive");
-            // -1/2 (1/m) IFFT(-K^2 FFT)/N^3 = IFFT(K^2 FFT) * (0.5/m/N^3)
-            f->coef[c] = 0.5 * (1.0 / m) / (double)p->nsites;
-        }
-        if (desc->potential == GP5_POT_HARMONIC) {
-            // (w_d * w_d * x * x) per axis and component (externalPotential.cpp:26)
-            double **tabs[3] = {&f->hx, &f->hy, &f->hz};
-            for (int d = 0; d < 3; d++) {
-                const int n = p->shape[d];
-                std::vector<double> h((size_t)n * p->ncomp);
-                for (int c = 0; c < p->ncomp; c++)
-                    for (int i = 0; i < n; i++) {
-                        const double w = desc->omegas[c][d], x = p->pos_host[d][i];
-                        h[(size_t)c * n + i] = w * w * x * x;
-                    }
-                check_cuda(cudaMalloc(tabs[d], sizeof(double) * h.size()), "cudaMalloc harmonic");
-                check_cuda(cudaMemcpy(*tabs[d], h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice),
-                           "upload harmonic");
-            }
-        }
+        f->sp_host = p->sp_host;
+        for (auto &S : f->sp_host) fill_functional_params(p, *desc, S);
+        upload_params(f->sp_host, &f->sp);
     } catch (...) {
         gp5cu_functional_destroy(f);
         throw;
@@ -524,9 +545,7 @@ int gp5cu_functional_destroy(gp5cu_functional *f) {
     if (!f) return GP5_OK;
     cudaSetDevice(f->plan->dev);
     cudaStreamSynchronize(f->plan->stream);
-    cudaFree(f->hx);
-    cudaFree(f->hy);
-    cudaFree(f->hz);
+    cudaFree(f->sp);
     delete f;
     return GP5_OK;
 }
@@ -549,11 +568,11 @@ int gp5cu_observables(gp5cu_functional *f, const void *field, gp5cu_observables_
     check_field_ptr(field, "field");
     gp5cu_plan *p = f->plan;
     use_device(p);
-    set_scalars(p->stream, p->ds);
+    set_scalars(p->stream, p->ds, p->nsolve);
     dispatch(p, [&](auto r) {
         // H psi lands in the workspace (read then written element by element by one thread)
         Launch<decltype(r)>::apply_h(f, field, p->work, true);
-        Launch<decltype(r)>::residual(p, field, p->work, p->ds);
+        Launch<decltype(r)>::residual(p, field, p->work, p->ds, f->sp);
     });
     double s[8];
     check_cuda(cudaMemcpyAsync(s, p->ds->sums, sizeof(s), cudaMemcpyDeviceToHost, p->stream), "read sums");
@@ -586,11 +605,17 @@ int gp5cu_stepper_create(gp5cu_functional *f, int kind, double dt, int imaginary
     st->tre = imaginary ? dt : 0.0;
     st->tim = imaginary ? 0.0 : dt;
     try {
-        check_cuda(cudaMalloc(&st->Ka, p->field_bytes), "cudaMalloc k buffers");
-        if (kind == GP5_STEP_RK4) check_cuda(cudaMalloc(&st->Kb, p->field_bytes), "cudaMalloc k buffers");
-        check_cuda(cudaMalloc(&st->ds, sizeof(DevScalars)), "cudaMalloc scalars");
-        check_cuda(cudaMemset(st->ds, 0, sizeof(DevScalars)), "memset scalars");
-        set_scalars(p->stream, st->ds);
+        check_cuda(cudaMalloc(&st->Ka, p->field_bytes * p->nsolve), "cudaMalloc k buffers");
+        if (kind == GP5_STEP_RK4) check_cuda(cudaMalloc(&st->Kb, p->field_bytes * p->nsolve), "cudaMalloc k buffers");
+        check_cuda(cudaMalloc(&st->ds, sizeof(DevScalars) * p->nsolve), "cudaMalloc scalars");
+        check_cuda(cudaMemset(st->ds, 0, sizeof(DevScalars) * p->nsolve), "memset scalars");
+        set_scalars(p->stream, st->ds, p->nsolve);
+        st->sp_host = f->sp_host;
+        for (auto &S : st->sp_host) {
+            S.tre = st->tre;
+            S.tim = st->tim;
+        }
+        upload_params(st->sp_host, &st->sp);
     } catch (...) {
         gp5cu_stepper_destroy(st);
         throw;
@@ -609,15 +634,18 @@ int gp5cu_stepper_destroy(gp5cu_stepper *st) {
     cudaFree(st->ds);
     cudaFree(st->phase_exp);
     cudaFree(st->dstate);
+    cudaFree(st->sp);
     delete st;
     return GP5_OK;
 }
 
-static void drop_graph(gp5cu_stepper *st) {
+extern "C++" {
+void drop_graph(gp5cu_stepper *st) {
     if (st->exec) cudaGraphExecDestroy(st->exec);
     st->exec = nullptr;
     st->graph_field = nullptr;
 }
+}  // extern "C++"
 
 int gp5cu_stepper_set_renormalization(gp5cu_stepper *st, int n, const double *N) {
     GP5_TRY
@@ -633,6 +661,11 @@ int gp5cu_stepper_set_renormalization(gp5cu_stepper *st, int n, const double *N)
         st->N[0] = N[0];
         st->N[1] = n > 1 ? N[1] : 0.0;
     }
+    for (auto &S : st->sp_host) {
+        S.Nt[0] = st->renorm ? st->N[0] : 0.0;
+        S.Nt[1] = st->renorm ? st->N[1] : 0.0;
+    }
+    upload_params(st->sp_host, &st->sp);
     drop_graph(st);
     GP5_CATCH
 }
@@ -658,19 +691,24 @@ int gp5cu_stepper_set_phase_constraint(gp5cu_stepper *st, const void *dphase) {
 
 // The merged stage-boundary path runs when one component is stepped and the x axis uses the
 // register engine; otherwise each stage is five passes with separate prologue/epilogue.
-static bool merged_path(const gp5cu_plan *p) { return p->ncomp == 1 && p->ax[0].reg; }
+extern "C++" {
+bool merged_path(const gp5cu_plan *p) { return p->ncomp == 1 && p->ax[0].reg; }
+}  // extern "C++"
 
-static int queue_step(gp5cu_stepper *st, void *field, bool merged, bool prologue) {
+extern "C++" {
+int queue_step(gp5cu_stepper *st, void *field, bool merged, bool prologue) {
     int n = 0;
     dispatch(st->func->plan, [&](auto r) {
         n = merged ? Launch<decltype(r)>::step_merged(st, field, prologue) : Launch<decltype(r)>::step(st, field);
     });
     return n;
 }
+}  // extern "C++"
 
-// Captures one step into a CUDA graph bound to this field; kernels are configured in a dry
+// Captures ksteps steps into a CUDA graph bound to this field; kernels are configured in a dry
 // pass first so that no attribute call happens during the capture.
-static void build_graph(gp5cu_stepper *st, void *field, bool merged) {
+extern "C++" {
+void build_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps) {
     gp5cu_plan *p = st->func->plan;
     drop_graph(st);
     p->dry = true;
@@ -685,7 +723,7 @@ static void build_graph(gp5cu_stepper *st, void *field, bool merged) {
     check_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     int n = 0;
     try {
-        n = queue_step(st, field, merged, false);
+        for (int k = 0; k < ksteps; k++) n = queue_step(st, field, merged, false);
     } catch (...) {
         cudaStreamEndCapture(p->stream, &g);
         if (g) cudaGraphDestroy(g);
@@ -697,8 +735,10 @@ static void build_graph(gp5cu_stepper *st, void *field, bool merged) {
     check_cuda(e, "cudaGraphInstantiate");
     st->graph_field = field;
     st->graph_merged = merged;
+    st->graph_steps = ksteps;
     st->launches_per_step = n;
 }
+}  // extern "C++"
 
 int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
     GP5_TRY
@@ -709,8 +749,9 @@ int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
     use_device(p);
     if (nsteps == 0) return GP5_OK;
     const bool merged = merged_path(p);
-    if (!st->exec || st->graph_field != field || st->graph_merged != merged) build_graph(st, field, merged);
-    set_scalars(p->stream, st->ds);
+    if (!st->exec || st->graph_field != field || st->graph_merged != merged || st->graph_steps != 1)
+        build_graph(st, field, merged, 1);
+    set_scalars(p->stream, st->ds, p->nsolve);
     if (merged) {
         // forward x transform of psi, consumed by the first graph step
         p->dry = false;
@@ -774,7 +815,7 @@ int gp5cu_stepper_profile(gp5cu_stepper *st, void *field, int nrep, double *ms, 
     ProfRec rec;
     p->prof = &rec;
     try {
-        set_scalars(p->stream, st->ds);
+        set_scalars(p->stream, st->ds, p->nsolve);
         const bool merged = merged_path(p);
         if (merged) {
             p->prof = nullptr;

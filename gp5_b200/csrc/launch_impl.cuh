@@ -22,13 +22,13 @@ inline TileGeom make_geom(const gp5cu_plan *p, int axis, int lines, bool pow2_bx
     g.axis = axis;
     g.n = p->shape[axis];
     g.estride = axis == 0 ? 1 : (axis == 1 ? (long long)g.nx : (long long)g.nx * g.ny);
+    long long tps = 0;
     if (axis == 0) {
         g.lines = lines;
         g.bx = g.bo = 1;
         g.tiles_x = 1;
         g.n_other = (long long)g.ny * g.nz * g.nc;
-        *tiles = (g.n_other + lines - 1) / lines;
-        g.ntiles = *tiles;
+        tps = (g.n_other + lines - 1) / lines;
     } else {
         int bx = std::min(lines, g.nx);
         if (pow2_bx) {
@@ -42,12 +42,15 @@ inline TileGeom make_geom(const gp5cu_plan *p, int axis, int lines, bool pow2_bx
         g.bo = bo;
         g.tiles_x = (g.nx + bx - 1) / bx;
         g.n_other = axis == 1 ? (long long)g.nz * g.nc : (long long)g.ny * g.nc;
-        *tiles = (long long)g.tiles_x * ((g.n_other + bo - 1) / bo);
-        g.ntiles = *tiles;
+        tps = (long long)g.tiles_x * ((g.n_other + bo - 1) / bo);
     }
+    g.nsolve = p->nsolve;
+    g.tiles_per_solve = tps;
+    g.solve_stride = p->solve_stride;
+    g.ntiles = tps * p->nsolve;
+    *tiles = g.ntiles;
     return g;
 }
-
 inline RedSlot red_slot(const gp5cu_plan *p) { return RedSlot{p->partials, p->counter}; }
 
 // Opt a kernel in to more than 48 KB of dynamic shared memory, once per (kernel, device,
@@ -120,9 +123,10 @@ void launch_axis(gp5cu_plan *p, int axis, const Op &op) {
     launch_smem<Real, CONTIG, MODE>(p, axis, op);
 }
 
+// Point-wise kernel over the sites of every solve: pw_bps blocks per solve.
 template <class Op> void launch_pointwise(gp5cu_plan *p, const Op &op) {
     if (p->dry) return;
-    k_pointwise<Op><<<p->pw_blocks, kThreads, 0, p->stream>>>(p->nsites, op, red_slot(p));
+    k_pointwise<Op><<<p->pw_bps * p->nsolve, kThreads, 0, p->stream>>>(p->nsites, p->pw_bps, op, red_slot(p));
     check_cuda(cudaGetLastError(), "k_pointwise launch");
     if (p->prof) p->prof->record(p->stream, 90);
 }
@@ -167,43 +171,37 @@ template <typename Real> void Launch<Real>::fft(gp5cu_plan *p, const void *src, 
     const V *s = (const V *)src;
     V *d = (V *)dst;
     if (dir == GP5_FORWARD) {
-        OpStageIn<Real, false> in{};
-        in.psi = s;
-        in.kprev = nullptr;
-        in.dst = d;
+        OpStageIn<Real, false> in{s, nullptr, d, p->ds, p->sp_lap, 0, 0.0, 1};
         launch_axis<Real, true, MODE_FWD>(p, 0, in);
-        OpCopy<Real> cp{d, d};
+        OpCopy<Real> cp{d, d, nullptr};
         launch_axis<Real, false, MODE_FWD>(p, 1, cp);
         launch_axis<Real, false, MODE_FWD>(p, 2, cp);
     } else {
-        OpCopy<Real> first{s, d};
+        OpCopy<Real> first{s, d, nullptr};
         launch_axis<Real, true, MODE_INV>(p, 0, first);
-        OpCopy<Real> cp{d, d};
+        OpCopy<Real> cp{d, d, nullptr};
         launch_axis<Real, false, MODE_INV>(p, 1, cp);
         launch_axis<Real, false, MODE_INV>(p, 2, cp);
     }
 }
 
+// x fwd, y fwd, z fwd * K^2 kin * z inv, y inv; the x inverse is left to the caller.
 template <typename Real>
-static void kinetic_passes(gp5cu_plan *p, const void *src, void *w, double coef0, double coef1) {
+static void kinetic_passes(gp5cu_plan *p, const void *src, void *w, const SolveParams *sp, DevScalars *ds) {
     using V = cpx<Real>;
-    OpStageIn<Real, false> in{};
-    in.psi = (const V *)src;
-    in.kprev = nullptr;
-    in.dst = (V *)w;
+    OpStageIn<Real, false> in{(const V *)src, nullptr, (V *)w, ds, sp, 0, 0.0, 1};
     launch_axis<Real, true, MODE_FWD>(p, 0, in);
-    OpCopy<Real> cp{(const V *)w, (V *)w};
+    OpCopy<Real> cp{(const V *)w, (V *)w, p->nsolve > 1 ? sp : nullptr};
     launch_axis<Real, false, MODE_FWD>(p, 1, cp);
-    OpKinetic<Real> kin{(const V *)w, (V *)w, p->k2[0], p->k2[1], p->k2[2], coef0, coef1, p->shape[2], p->dk[2]};
+    OpKinetic<Real> kin{(const V *)w, (V *)w, sp, p->shape[0], p->shape[1], p->shape[2]};
     launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
     launch_axis<Real, false, MODE_INV>(p, 1, cp);
 }
 
 template <typename Real> void Launch<Real>::laplacian(gp5cu_plan *p, const void *src, void *dst) {
     using V = cpx<Real>;
-    const double c = -1.0 / (double)p->nsites;
-    kinetic_passes<Real>(p, src, p->work, c, c);
-    OpCopy<Real> last{(const V *)p->work, (V *)dst};
+    kinetic_passes<Real>(p, src, p->work, p->sp_lap, p->ds);
+    OpCopy<Real> last{(const V *)p->work, (V *)dst, nullptr};
     launch_axis<Real, true, MODE_INV>(p, 0, last);
 }
 
@@ -214,23 +212,12 @@ template <typename Real> static EpiParams<Real> base_epi(gp5cu_functional *f) {
     P.nsites = p->nsites;
     P.fkind = d.kind;
     P.has_g = d.has_couplings;
-    P.g00 = (Real)d.couplings[0];
-    P.g01 = (Real)d.couplings[1];
-    P.g11 = (Real)d.couplings[3];
-    P.c3 = (Real)d.c3;
-    P.c4 = (Real)d.c4;
-    P.la = (Real)d.alpha;
-    P.lb = (Real)d.beta;
-    P.le = (Real)d.eta;
     P.pot = d.potential;
-    P.hx = f->hx;
-    P.hy = f->hy;
-    P.hz = f->hz;
     P.nx = p->shape[0];
     P.ny = p->shape[1];
     P.nz = p->shape[2];
     P.varr = (const Real *)d.dpotential;
-    P.dV = p->dV;
+    P.sp = f->sp;
     return P;
 }
 
@@ -246,12 +233,12 @@ static void epilogue(gp5cu_plan *p, const EpiParams<Real> &P, bool red) {
             launch_axis<Real, true, MODE_INV>(p, 0, op);
         }
     } else {
-        OpCopy<Real> cp{(const V *)p->work, (V *)p->work};
+        OpCopy<Real> cp{(const V *)p->work, (V *)p->work, P.sp};
         launch_axis<Real, true, MODE_INV>(p, 0, cp);
         EpiParams<Real> Q = P;
         Q.tsrc = (const V *)p->work;
-        if (red) launch_pointwise(p, OpSiteEpilogue<Real, 2, true>{Q});
-        else launch_pointwise(p, OpSiteEpilogue<Real, 2, false>{Q});
+        if (red) launch_pointwise(p, OpSiteEpilogue<Real, 2, true>{Q, p->solve_stride});
+        else launch_pointwise(p, OpSiteEpilogue<Real, 2, false>{Q, p->solve_stride});
     }
 }
 
@@ -259,7 +246,7 @@ template <typename Real>
 void Launch<Real>::apply_h(gp5cu_functional *f, const void *src, void *dst, bool obs) {
     using V = cpx<Real>;
     gp5cu_plan *p = f->plan;
-    kinetic_passes<Real>(p, src, p->work, f->coef[0], f->coef[1]);
+    kinetic_passes<Real>(p, src, p->work, f->sp, p->ds);
     EpiParams<Real> P = base_epi<Real>(f);
     P.mode = obs ? EPI_OBS : EPI_H;
     P.psi = (const V *)src;
@@ -269,53 +256,53 @@ void Launch<Real>::apply_h(gp5cu_functional *f, const void *src, void *dst, bool
 }
 
 template <typename Real>
-void Launch<Real>::residual(gp5cu_plan *p, const void *psi, const void *hpsi, DevScalars *ds) {
+void Launch<Real>::residual(gp5cu_plan *p, const void *psi, const void *hpsi, DevScalars *ds, const SolveParams *sp) {
     using V = cpx<Real>;
-    OpResidual<Real> op{(const V *)psi, (const V *)hpsi, p->nsites, p->ncomp, ds};
+    OpResidual<Real> op{(const V *)psi, (const V *)hpsi, p->nsites, p->solve_stride, p->ncomp, ds, sp};
     launch_pointwise(p, op);
 }
 
 template <typename Real>
 void Launch<Real>::norm(gp5cu_plan *p, const void *field, int comp, double Ntarget, DevScalars *ds) {
     using V = cpx<Real>;
-    OpNorm<Real> op{(const V *)field, p->nsites, comp, p->ncomp, ds, Ntarget, p->dV};
+    OpNorm<Real> op{(const V *)field, p->nsites, p->solve_stride, comp, p->ncomp, ds, Ntarget, p->dV};
     launch_pointwise(p, op);
 }
 
 template <typename Real>
 void Launch<Real>::scale(gp5cu_plan *p, void *field, int comp, DevScalars *ds, bool from_sigma) {
     using V = cpx<Real>;
-    OpScale<Real> op{(V *)field, p->nsites, comp, p->ncomp, ds, from_sigma ? 1 : 0};
+    OpScale<Real> op{(V *)field, p->nsites, p->solve_stride, comp, p->ncomp, ds, from_sigma ? 1 : 0};
     launch_pointwise(p, op);
 }
 
 template <typename Real> void Launch<Real>::max_density(gp5cu_plan *p, const void *field) {
     check_cuda(cudaMemsetAsync(p->dmax, 0, sizeof(unsigned long long), p->stream), "memset");
-    k_max_density<Real><<<p->pw_blocks, kThreads, 0, p->stream>>>((const cpx<Real> *)field, p->nsites,
-                                                                    p->ncomp, p->dmax);
+    k_max_density<Real><<<p->pw_blocks, kThreads, 0, p->stream>>>((const cpx<Real> *)field,
+                                                                    p->nsites * p->nsolve, p->ncomp, p->dmax);
     check_cuda(cudaGetLastError(), "k_max_density launch");
 }
 
 template <typename Real>
-void Launch<Real>::convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128) {
+void Launch<Real>::convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128,
+                           long long n) {
     OpConvert<Real> op{(const double2 *)in128, (cpx<Real> *)out, (const cpx<Real> *)in, (double2 *)out128};
-    k_pointwise<OpConvert<Real>><<<p->pw_blocks, kThreads, 0, p->stream>>>(p->nsites * p->ncomp, op,
-                                                                           red_slot(p));
+    k_pointwise<OpConvert<Real>><<<p->pw_blocks, kThreads, 0, p->stream>>>(n, p->pw_blocks, op, red_slot(p));
     check_cuda(cudaGetLastError(), "convert launch");
 }
 
 template <typename Real> void Launch<Real>::phase_exp(gp5cu_plan *p, const void *phase, void *out) {
     k_phase_exp<Real><<<p->pw_blocks, kThreads, 0, p->stream>>>((const Real *)phase, (cpx<Real> *)out,
-                                                                 p->nsites * p->ncomp);
+                                                                 p->nsites * p->ncomp * p->nsolve);
     check_cuda(cudaGetLastError(), "phase_exp launch");
 }
 
 // ---- one stepper step ----------------------------------------------------------------------
-// RK4 (stepper.cpp:46-71) as four stages of five axis passes each:
+// Five-pass form (RK4, stepper.cpp:46-71): four stages of
 //   x fwd [u~ = sigma psi0 - c k_{s-1}, |u~|^2]  y fwd  z fwd*K^2/(2mN^3)*z inv  y inv
 //   x inv [k_s = H(alpha u~); RK bookkeeping; psi1 on the last stage]
 // Buffers: psi (in/out, in place), work (transform), Ka (k1, then the running sum
-// k1 + 2k2 + 2k3), Kb (k2, then k3).
+// k1 + 2k2 + 2k3), Kb (k2, then k3).  Used when the stage boundary cannot be merged.
 template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) {
     using V = cpx<Real>;
     gp5cu_functional *f = st->func;
@@ -328,30 +315,29 @@ template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) 
     const int nst = rk4 ? 4 : 1;
     int launches = 0;
     for (int s = 1; s <= nst; s++) {
-        double cre = 0, cim = 0;
+        double cfac = 0;
         const V *kprev = nullptr;
         if (rk4 && s > 1) {
-            const double a = (s == 4) ? 1.0 : 0.5;
-            cre = st->tre * a;
-            cim = st->tim * a;
+            cfac = (s == 4) ? 1.0 : 0.5;
             kprev = (s == 2) ? Ka : Kb;
         }
         const bool red_in = st->renorm && rk4 && s > 1;
         if (red_in) {
-            OpStageIn<Real, true> in{psi, kprev, W, st->ds, 1, (Real)cre, (Real)cim, st->N[0], st->N[1], p->dV, s & 1};
+            OpStageIn<Real, true> in{psi, kprev, W, st->ds, st->sp, 1, cfac, s & 1};
             launch_axis<Real, true, MODE_FWD>(p, 0, in);
         } else {
-            OpStageIn<Real, false> in{psi, kprev, W, st->ds, st->renorm ? 1 : 0, (Real)cre, (Real)cim, 0, 0, p->dV, s & 1};
+            OpStageIn<Real, false> in{psi, kprev, W, st->ds, st->sp, st->renorm ? 1 : 0, cfac, s & 1};
             launch_axis<Real, true, MODE_FWD>(p, 0, in);
         }
-        OpCopy<Real> cp{W, W};
+        OpCopy<Real> cp{W, W, p->nsolve > 1 ? st->sp : nullptr};  // only a batch needs the active flags
         launch_axis<Real, false, MODE_FWD>(p, 1, cp);
-        OpKinetic<Real> kin{W, W, p->k2[0], p->k2[1], p->k2[2], f->coef[0], f->coef[1], p->shape[2], p->dk[2]};
+        OpKinetic<Real> kin{W, W, st->sp, p->shape[0], p->shape[1], p->shape[2]};
         launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
         launch_axis<Real, false, MODE_INV>(p, 1, cp);
         launches += 4;
 
         EpiParams<Real> P = base_epi<Real>(f);
+        P.sp = st->sp;
         P.ds = st->ds;
         P.psi = psi;
         P.psi_out = psi;
@@ -360,25 +346,20 @@ template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) 
         P.use_sigma = st->renorm ? 1 : 0;
         P.use_alpha = red_in ? 1 : 0;
         P.slot = s & 1;
-        P.cre = (Real)cre;
-        P.cim = (Real)cim;
+        P.cfac = cfac;
         P.phase_exp = nullptr;
         if (!rk4) {
             P.mode = EPI_EULER;
-            P.dre = (Real)st->tre;
-            P.dim = (Real)st->tim;
+            P.dfac = 1.0;
         } else {
             P.mode = EPI_RK1 + (s - 1);
             P.kout = (s == 1) ? Ka : Kb;
-            P.dre = (Real)(st->tre * (1. / 6));
-            P.dim = (Real)(st->tim * (1. / 6));
+            P.dfac = 1. / 6;
         }
         const bool last = (s == nst);
         if (last) {
             P.phase_exp = (const V *)st->phase_exp;
             P.renorm_out = st->renorm ? 1 : 0;
-            P.Nt0 = st->N[0];
-            P.Nt1 = st->N[1];
         }
         epilogue<Real>(p, P, last && st->renorm);
         launches += (p->ncomp == 1) ? 1 : 2;
@@ -386,18 +367,18 @@ template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) 
     return launches;
 }
 
+template <typename Real> void Launch<Real>::prologue(gp5cu_stepper *st, void *field) {
+    using V = cpx<Real>;
+    gp5cu_plan *p = st->func->plan;
+    OpStageIn<Real, false> in{(const V *)field, nullptr, (V *)p->work, st->ds, st->sp, 0, 0.0, 1};
+    launch_axis<Real, true, MODE_FWD>(p, 0, in);
+}
+
 // RK4 / Euler with the stage boundaries merged: after the prologue transform of psi (once
 // per advance call), every stage is y fwd, z fwd*K^2/(2mN^3)*z inv, y inv, then one x kernel
 // that inverts x, finishes stage s (k_s, RK bookkeeping, psi1 after the last stage), forms the
 // input of the next stage (u~_{s+1} = sigma psi0 - c_{s+1} k_s, or psi1) and transforms it
 // forward in x.  Field transfers per RK4 step: 47 instead of 54; 16 launches instead of 20.
-template <typename Real> void Launch<Real>::prologue(gp5cu_stepper *st, void *field) {
-    using V = cpx<Real>;
-    gp5cu_plan *p = st->func->plan;
-    OpStageIn<Real, false> in{(const V *)field, nullptr, (V *)p->work, st->ds, 0, (Real)0, (Real)0, 0, 0, p->dV, 1};
-    launch_axis<Real, true, MODE_FWD>(p, 0, in);
-}
-
 template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *field, bool prologue) {
     using V = cpx<Real>;
     gp5cu_functional *f = st->func;
@@ -413,18 +394,14 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
         Launch<Real>::prologue(st, field);
         launches++;
     }
-    auto coef = [&](int stage, double &re, double &im) {  // u~_stage = sigma psi0 - coef k_{stage-1}
-        const double a = (stage == 4) ? 1.0 : 0.5;
-        re = st->tre * a;
-        im = st->tim * a;
-    };
     for (int s = 1; s <= nst; s++) {
-        OpCopy<Real> cp{W, W};
+        OpCopy<Real> cp{W, W, p->nsolve > 1 ? st->sp : nullptr};  // only a batch needs the active flags
         launch_axis<Real, false, MODE_FWD>(p, 1, cp);
-        OpKinetic<Real> kin{W, W, p->k2[0], p->k2[1], p->k2[2], f->coef[0], f->coef[1], p->shape[2], p->dk[2]};
+        OpKinetic<Real> kin{W, W, st->sp, p->shape[0], p->shape[1], p->shape[2]};
         launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
         launch_axis<Real, false, MODE_INV>(p, 1, cp);
         EpiParams<Real> P = base_epi<Real>(f);
+        P.sp = st->sp;
         P.ds = st->ds;
         P.psi = psi;
         P.psi_out = psi;
@@ -435,30 +412,21 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
         P.u1_raw = (s == 1) ? 1 : 0;
         P.turn = 1;
         P.renorm_out = st->renorm ? 1 : 0;
-        P.Nt0 = st->N[0];
-        P.Nt1 = st->N[1];
         P.phase_exp = nullptr;
-        double cre = 0, cim = 0, cnre = 0, cnim = 0;
         if (!rk4) {
             P.mode = EPI_EULER;
             P.kprev = nullptr;
-            P.dre = (Real)st->tre;
-            P.dim = (Real)st->tim;
+            P.dfac = 1.0;
             P.phase_exp = (const V *)st->phase_exp;
         } else {
             P.mode = EPI_RK1 + (s - 1);
             P.kprev = (s == 1) ? nullptr : ((s == 2) ? Ka : Kb);
             P.kout = (s == 1) ? Ka : Kb;
-            P.dre = (Real)(st->tre * (1. / 6));
-            P.dim = (Real)(st->tim * (1. / 6));
-            if (s > 1) coef(s, cre, cim);
-            if (s < 4) coef(s + 1, cnre, cnim);
+            P.dfac = 1. / 6;
+            P.cfac = (s == 1) ? 0.0 : ((s == 4) ? 1.0 : 0.5);      // u~_s = sigma psi0 - tau cfac k_{s-1}
+            P.cnfac = (s < 4) ? ((s + 1 == 4) ? 1.0 : 0.5) : 0.0;  // u~_{s+1}
             if (s == 4) P.phase_exp = (const V *)st->phase_exp;
         }
-        P.cre = (Real)cre;
-        P.cim = (Real)cim;
-        P.cnre = (Real)cnre;
-        P.cnim = (Real)cnim;
         if (st->renorm) {
             OpStageOut<Real, true, true> op{W, P};
             launch_axis<Real, true, MODE_INV_TURN_FWD>(p, 0, op);

@@ -32,24 +32,30 @@ struct TileGeom {
     int bx, bo;         // strided tiles: consecutive x lines, other lines
     int tiles_x;        // strided tiles: ceil(nx / bx)
     long long n_other;  // strided: number of (other) line groups; x axis: total lines
-    long long ntiles;   // tiles of the pass (a persistent CTA walks tile += gridDim.x)
+    long long ntiles;   // tiles of the launch: nsolve * tiles_per_solve
+    int nsolve;                 // independent solves of this grid in the launch
+    long long tiles_per_solve;  // tiles of one solve (consecutive tile indices)
+    long long solve_stride;     // elements between the fields of consecutive solves
 };
 
 struct RedSlot {
-    double *partials;   // [gridDim.x * 8]
-    unsigned *counter;  // zero between launches
+    double *partials;   // [nsolve][tiles_per_solve][8]
+    unsigned *counter;  // [nsolve], zero between launches
 };
 
-// Coordinates of one line: base offset and the fixed coordinates.
+// Coordinates of one line: base offset (including the solve's offset) and fixed coordinates.
 struct LineRef {
     long long base;
     int i, j, k, c;
+    int solve;
     bool valid;
 };
 
-__device__ __forceinline__ LineRef line_ref(const TileGeom &g, long long tile, int line) {
+__device__ __forceinline__ LineRef line_ref(const TileGeom &g, long long tile_all, int line) {
     LineRef r;
     r.i = r.j = r.k = r.c = 0;
+    r.solve = (int)(tile_all / g.tiles_per_solve);
+    const long long tile = tile_all - (long long)r.solve * g.tiles_per_solve;
     if (g.axis == 0) {
         long long L = tile * g.lines + line;
         r.valid = L < g.n_other;
@@ -77,6 +83,7 @@ __device__ __forceinline__ LineRef line_ref(const TileGeom &g, long long tile, i
             r.base = i + (long long)g.nx * r.j + (long long)g.nx * g.ny * g.nz * r.c;
         }
     }
+    r.base += (long long)r.solve * g.solve_stride;
     return r;
 }
 
@@ -121,32 +128,34 @@ __device__ __forceinline__ void neumaier(double &s, double &comp, double x) {
     s = t;
 }
 
-// Per-block partials, then the last block folds them and calls op.finalize(sums).
+// Per-block partials, then the last block of the solve folds that solve's partials and calls
+// op.finalize(sums, solve).  lb = block index within the solve, nb = blocks of the solve.
 template <int K, class Op>
-__device__ void reduce_and_finalize(const double *acc_in, const RedSlot &rs, const Op &op) {
+__device__ void reduce_and_finalize(const double *acc_in, const RedSlot &rs, const Op &op, int solve,
+                                    long long lb, long long nb) {
     if constexpr (K > 0) {
         double acc[K];
 #pragma unroll
         for (int r = 0; r < K; r++) acc[r] = acc_in[r];
         block_sum<K>(acc);
-        const long long nblocks = (long long)gridDim.x;
+        double *part = rs.partials + (long long)solve * nb * K;
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int r = 0; r < K; r++) rs.partials[(long long)blockIdx.x * K + r] = acc[r];
+            for (int r = 0; r < K; r++) part[lb * K + r] = acc[r];
         }
         __threadfence();
         __shared__ bool s_last;
         __syncthreads();
-        if (threadIdx.x == 0) s_last = (atomicAdd(rs.counter, 1u) == (unsigned)(nblocks - 1));
+        if (threadIdx.x == 0) s_last = (atomicAdd(rs.counter + solve, 1u) == (unsigned)(nb - 1));
         __syncthreads();
         if (s_last) {
             __threadfence();
             double s[K], cp[K];
 #pragma unroll
             for (int r = 0; r < K; r++) { s[r] = 0.0; cp[r] = 0.0; }
-            for (long long b = threadIdx.x; b < nblocks; b += blockDim.x) {
+            for (long long b = threadIdx.x; b < nb; b += blockDim.x) {
 #pragma unroll
-                for (int r = 0; r < K; r++) neumaier(s[r], cp[r], __ldcg(rs.partials + b * K + r));
+                for (int r = 0; r < K; r++) neumaier(s[r], cp[r], __ldcg(part + b * K + r));
             }
             block_sum<K>(s);
             block_sum<K>(cp);
@@ -154,8 +163,8 @@ __device__ void reduce_and_finalize(const double *acc_in, const RedSlot &rs, con
                 double tot[K];
 #pragma unroll
                 for (int r = 0; r < K; r++) tot[r] = s[r] + cp[r];
-                op.finalize(tot);
-                *rs.counter = 0u;
+                op.finalize(tot, solve);
+                rs.counter[solve] = 0u;
             }
         }
     }
@@ -179,10 +188,11 @@ __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, 
     const void *st[4];
     const int ns = op.streams(st);
     if (ns < 2 || threadIdx.x != 0 || g.axis != 0) return;
-    const long long L0 = tile * g.lines;
+    const long long solve = tile / g.tiles_per_solve, lt = tile - solve * g.tiles_per_solve;
+    const long long L0 = lt * g.lines;
     long long L1 = L0 + g.lines;
     if (L1 > g.n_other) L1 = g.n_other;
-    const long long e0 = L0 * g.nx, cnt = (L1 - L0) * g.nx;
+    const long long e0 = solve * g.solve_stride + L0 * g.nx, cnt = (L1 - L0) * g.nx;
     for (int q = 0; q < ns; q++)
         prefetch_l2(reinterpret_cast<const V *>(st[q]) + e0, (unsigned)(cnt * sizeof(V)));
 }
@@ -223,40 +233,64 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
 #pragma unroll
     for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); r++) acc[r] = 0.0;
 
-    if (CONTIG) prefetch_aux<V>(g, blockIdx.x, op);
+    const long long tile = blockIdx.x;
+    const int solve = (int)(tile / g.tiles_per_solve);
+    __shared__ typename Op::Ctx X;
+    const void *streams[4];
+    op.streams(streams);
+    const V *__restrict__ src0 = reinterpret_cast<const V *>(streams[0]);
+    if (CONTIG) prefetch_aux<V>(g, tile, op);
     {
-        const long long tile = blockIdx.x;
         LineRef lr = line_ref(g, tile, line);
+        // the solve's context and the tile's first stream are fetched together
+        const unsigned long long cw = ctx_fetch(op.params(), op.scalars(), solve);
         V v[E];
 #pragma unroll
-        for (int m = 0; m < E; m++) {
-            const int pos = tid + T * m;
-            if (lr.valid) {
+        for (int m = 0; m < E; m++)
+            v[m] = lr.valid ? src0[lr.base + (tid + T * m) * g.estride] : mk<Real>(0, 0);
+        if (op.params() || op.scalars()) {  // uniform: ops without per-solve data skip the barrier
+            ctx_store(X, op.params(), op.scalars(), cw);
+            __syncthreads();
+            if (op.params() && !X.S.active) return;  // a finished solve's tiles return at once
+        }
+        if (lr.valid) {
+#pragma unroll
+            for (int m = 0; m < E; m++) {
+                const int pos = tid + T * m;
                 LineRef e = lr;
                 set_pos(g, e, pos);
-                v[m] = op.load(lr.base + pos * g.estride, e, acc);
-            } else {
-                v[m] = mk<Real>(0, 0);
+                const long long ge = lr.base + pos * g.estride;
+                v[m] = op.load(v[m], ge, e, acc, X);
             }
         }
         if constexpr (MODE == MODE_INV_TURN_FWD) {
             static_assert(CONTIG, "the stage boundary runs on x lines");
             LayContig<N> lay;
             reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+            // The epilogue/prologue runs as a rolled loop over the thread's own elements staged
+            // in shared memory: one copy of its code (the unrolled form overflowed the
+            // instruction cache) and the transform registers are free meanwhile.  Each thread
+            // reads back only what it wrote, so no barrier is needed around the loop.
 #pragma unroll
-            for (int m0 = 0; m0 < E; m0 += NB) {
-                typename Op::Pre pre[NB];
+            for (int m = 0; m < E; m++) sm[lay(line, tid + T * m)] = v[m];
+            if (lr.valid) {
+#pragma unroll 1
+                for (int m0 = 0; m0 < E; m0 += NB) {
+                    typename Op::Pre pre[NB];
 #pragma unroll
-                for (int j = 0; j < NB; j++)
-                    pre[j] = lr.valid ? op.pre(lr.base + (tid + T * (m0 + j)) * g.estride) : typename Op::Pre{};
+                    for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * g.estride);
 #pragma unroll
-                for (int j = 0; j < NB; j++) {
-                    const int pos = tid + T * (m0 + j);
-                    LineRef e = lr;
-                    set_pos(g, e, pos);
-                    if (lr.valid) v[m0 + j] = op.turn(lr.base + pos * g.estride, e, v[m0 + j], pre[j], acc);
+                    for (int j = 0; j < NB; j++) {
+                        const int pos = tid + T * (m0 + j);
+                        LineRef e = lr;
+                        set_pos(g, e, pos);
+                        const int si = lay(line, pos);
+                        sm[si] = op.turn(lr.base + pos * g.estride, e, sm[si], pre[j], acc, X);
+                    }
                 }
             }
+#pragma unroll
+            for (int m = 0; m < E; m++) v[m] = sm[lay(line, tid + T * m)];
             __syncthreads();
             reg_fft<N, -1>(v, tid, line, tw, sm, lay);
         } else if constexpr (CONTIG) {
@@ -268,7 +302,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 for (int m = 0; m < E; m++) {
                     LineRef e = lr;
                     set_pos(g, e, tid + T * m);
-                    v[m] = op.mid(v[m], e);
+                    v[m] = op.mid(v[m], e, X);
                 }
                 __syncthreads();  // also a scheduling fence: keeps register pressure below 128
                 reg_fft<N, 1>(v, tid, line, tw, sm, lay);
@@ -282,7 +316,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 for (int m = 0; m < E; m++) {
                     LineRef e = lr;
                     set_pos(g, e, tid + T * m);
-                    v[m] = op.mid(v[m], e);
+                    v[m] = op.mid(v[m], e, X);
                 }
                 __syncthreads();  // also a scheduling fence: keeps register pressure below 128
                 reg_fft<N, 1>(v, tid, line, tw, sm, lay);
@@ -294,7 +328,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 const int pos = tid + T * m;
                 LineRef e = lr;
                 set_pos(g, e, pos);
-                op.post(lr.base + pos * g.estride, e, v[m], typename Op::Pre{}, acc);
+                op.post(lr.base + pos * g.estride, e, v[m], typename Op::Pre{}, acc, X);
             }
         } else if (lr.valid) {
             // epilogue in batches: the operand loads of NB elements are issued together
@@ -308,12 +342,13 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                     const int pos = tid + T * (m0 + j);
                     LineRef e = lr;
                     set_pos(g, e, pos);
-                    op.post(lr.base + pos * g.estride, e, v[m0 + j], pre[j], acc);
+                    op.post(lr.base + pos * g.estride, e, v[m0 + j], pre[j], acc, X);
                 }
             }
         }
     }
-    reduce_and_finalize<Op::NRED>(acc, rs, op);
+    reduce_and_finalize<Op::NRED>(acc, rs, op, solve, tile - (long long)solve * g.tiles_per_solve,
+                                  g.tiles_per_solve);
 }
 
 // ---- shared-memory-engine kernel (any length) ---------------------------------------------
@@ -338,17 +373,27 @@ k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__r
 #pragma unroll
     for (int r = 0; r < K; r++) acc[r] = 0.0;
 
+    const long long tile = blockIdx.x;
+    const int solve = (int)(tile / g.tiles_per_solve);
+    __shared__ typename Op::Ctx X;
+    load_ctx(X, op.params(), op.scalars(), solve);
+    __syncthreads();
+    if (op.params() && !X.S.active) return;
+    const void *streams[4];
+    op.streams(streams);
+    const V *__restrict__ src0 = reinterpret_cast<const V *>(streams[0]);
     auto lay_idx = [&](int line, int pos) { return CONTIG ? line * ld + pos : pos * lines + line; };
     const int total = lines * n;
     for (int q = threadIdx.x; q < total; q += blockDim.x) {
         int line, pos;
         if (CONTIG) { pos = q % n; line = q / n; }
         else { line = q % lines; pos = q / lines; }
-        LineRef lr = line_ref(g, blockIdx.x, line);
+        LineRef lr = line_ref(g, tile, line);
         V val = mk<Real>(0, 0);
         if (lr.valid) {
             set_pos(g, lr, pos);
-            val = op.load(lr.base + pos * g.estride, lr, acc);
+            const long long ge = lr.base + pos * g.estride;
+            val = op.load(src0[ge], ge, lr, acc, X);
         }
         b0[lay_idx(line, pos)] = val;
     }
@@ -368,10 +413,10 @@ k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__r
             int line, pos;
             if (CONTIG) { pos = q % n; line = q / n; }
             else { line = q % lines; pos = q / lines; }
-            LineRef lr = line_ref(g, blockIdx.x, line);
+            LineRef lr = line_ref(g, tile, line);
             set_pos(g, lr, pos);
             const int s = lay_idx(line, pos);
-            res[s] = op.mid(res[s], lr);
+            res[s] = op.mid(res[s], lr, X);
         }
         __syncthreads();
         V *other = (res == b0) ? b1 : b0;
@@ -387,28 +432,36 @@ k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__r
         int line, pos;
         if (CONTIG) { pos = q % n; line = q / n; }
         else { line = q % lines; pos = q / lines; }
-        LineRef lr = line_ref(g, blockIdx.x, line);
+        LineRef lr = line_ref(g, tile, line);
         if (lr.valid) {
             set_pos(g, lr, pos);
             const long long ge = lr.base + pos * g.estride;
             const typename Op::Pre pre = op.pre(ge);
-            op.post(ge, lr, res[lay_idx(line, pos)], pre, acc);
+            op.post(ge, lr, res[lay_idx(line, pos)], pre, acc, X);
         }
     }
-    reduce_and_finalize<Op::NRED>(acc, rs, op);
+    reduce_and_finalize<Op::NRED>(acc, rs, op, solve, tile - (long long)solve * g.tiles_per_solve,
+                                  g.tiles_per_solve);
 }
 
 // ---- point-wise kernel over all sites (reductions, scaling, conversions) -----------------
+// Grid: nsolve * bps blocks; block b works on solve b / bps, sites of that solve strided by
+// bps * blockDim.x.
 template <class Op>
-__global__ void __launch_bounds__(256) k_pointwise(const long long nsites, Op op, const RedSlot rs) {
+__global__ void __launch_bounds__(256) k_pointwise(const long long nsites, const int bps, Op op, const RedSlot rs) {
     constexpr int K = Op::NRED > 0 ? Op::NRED : 1;
+    const int solve = blockIdx.x / bps;
+    const int lb = blockIdx.x - solve * bps;
+    __shared__ typename Op::Ctx X;
+    load_ctx(X, op.params(), op.scalars(), solve);
+    __syncthreads();
+    if (op.params() && !X.S.active) return;
     double acc[K];
 #pragma unroll
     for (int r = 0; r < K; r++) acc[r] = 0.0;
-    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsites;
-         s += (long long)gridDim.x * blockDim.x)
-        op.site(s, acc);
-    reduce_and_finalize<Op::NRED>(acc, rs, op);
+    for (long long s = (long long)lb * blockDim.x + threadIdx.x; s < nsites; s += (long long)bps * blockDim.x)
+        op.site(solve, s, acc, X);
+    reduce_and_finalize<Op::NRED>(acc, rs, op, solve, lb, bps);
 }
 
 }  // namespace gp5

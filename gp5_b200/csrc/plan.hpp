@@ -41,6 +41,9 @@ void check_cuda(cudaError_t e, const char *what);
 
 }  // namespace gp5
 
+gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const double *const *rights, int nsolve,
+                        int ncomp, int precision, int device);
+
 struct gp5cu_plan {
     int dev = 0;
     int shape[3] = {0, 0, 0};
@@ -48,22 +51,24 @@ struct gp5cu_plan {
     int ncomp = 1;
     int prec = GP5_C128;
     long long nsites = 0;  // nx*ny*nz
+    int nsolve = 1;              // independent solves of this grid carried by every launch
+    long long solve_stride = 0;  // elements between consecutive solves' fields (nsites*ncomp)
     size_t elem_bytes = 16;
     size_t field_bytes = 0;
     double dV = 1.0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
     gp5::AxisPlan ax[3];
-    double *k2[3] = {nullptr, nullptr, nullptr};  // device k_d^2
-    double dk[3] = {0, 0, 0};                     // Fourier steps 2 pi / L_d
-    std::vector<double> pos_host[3];              // cell-centred coordinates
     void *work = nullptr;                         // one field of FFT workspace
     double *partials = nullptr;
     unsigned *counter = nullptr;
     long long max_blocks = 0;
-    gp5::DevScalars *ds = nullptr;
+    gp5::DevScalars *ds = nullptr;         // [nsolve]
+    gp5::SolveParams *sp_lap = nullptr;    // [nsolve]: geometry, kinetic factor -1/N^3
+    std::vector<gp5::SolveParams> sp_host; // [nsolve]: geometry of every solve
     unsigned long long *dmax = nullptr;
-    int pw_blocks = 0;  // grid of the point-wise kernels
+    int pw_blocks = 0;  // grid of the single-solve point-wise kernels
+    int pw_bps = 0;     // point-wise blocks per solve
     int sms = 148;      // multiprocessors of the device
     gp5::ProfRec *prof = nullptr;
     bool dry = false;  // launch helpers only configure kernels (before a stream capture)
@@ -72,8 +77,8 @@ struct gp5cu_plan {
 struct gp5cu_functional {
     gp5cu_plan *plan = nullptr;
     gp5cu_functional_desc desc{};
-    double *hx = nullptr, *hy = nullptr, *hz = nullptr;  // harmonic tables [ncomp][n_d]
-    double coef[2] = {0, 0};                            // kinetic multiplier per component
+    std::vector<gp5::SolveParams> sp_host;  // [nsolve]
+    gp5::SolveParams *sp = nullptr;         // device copy
 };
 
 struct gp5cu_stepper {
@@ -87,10 +92,13 @@ struct gp5cu_stepper {
     void *phase_exp = nullptr;  // e^{i phi}, plan precision, owned
     void *Ka = nullptr, *Kb = nullptr;
     void *dstate = nullptr;  // resident state of the host-buffer entry point
-    gp5::DevScalars *ds = nullptr;
+    gp5::DevScalars *ds = nullptr;          // [nsolve]
+    std::vector<gp5::SolveParams> sp_host;  // [nsolve]: functional + time step + targets
+    gp5::SolveParams *sp = nullptr;
     cudaGraphExec_t exec = nullptr;
     void *graph_field = nullptr;
     bool graph_merged = false;
+    int graph_steps = 0;
     double t = 0;
     int launches_per_step = 0;
 };
@@ -102,18 +110,27 @@ template <typename Real> struct Launch {
     static void fft(gp5cu_plan *p, const void *src, void *dst, int dir);
     static void laplacian(gp5cu_plan *p, const void *src, void *dst);
     static void apply_h(gp5cu_functional *f, const void *src, void *dst, bool obs);
-    static void residual(gp5cu_plan *p, const void *psi, const void *hpsi, DevScalars *ds);
+    static void residual(gp5cu_plan *p, const void *psi, const void *hpsi, DevScalars *ds, const SolveParams *sp);
     static void norm(gp5cu_plan *p, const void *field, int comp, double Ntarget, DevScalars *ds);
     static void scale(gp5cu_plan *p, void *field, int comp, DevScalars *ds, bool from_sigma);
     static void max_density(gp5cu_plan *p, const void *field);
-    static void convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128);
+    static void convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128, long long n);
     static int step(gp5cu_stepper *st, void *field);  // queue one step; returns launches
     static int step_merged(gp5cu_stepper *st, void *field, bool prologue);
     static void prologue(gp5cu_stepper *st, void *field);  // forward x transform of psi
     static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
 };
 
-void set_scalars(cudaStream_t s, DevScalars *ds);
+void set_scalars(cudaStream_t s, DevScalars *ds, int n = 1);
+
 void build_axis_plan(gp5cu_plan *p, int d);
 
 }  // namespace gp5
+
+// host helpers shared by the single-solve and batched entry points (gp5cu_host.cu)
+void fill_functional_params(const gp5cu_plan *p, const gp5cu_functional_desc &d, gp5::SolveParams &S);
+void upload_params(const std::vector<gp5::SolveParams> &h, gp5::SolveParams **dptr);
+bool merged_path(const gp5cu_plan *p);
+int queue_step(gp5cu_stepper *st, void *field, bool merged, bool prologue);
+void build_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps);
+void drop_graph(gp5cu_stepper *st);

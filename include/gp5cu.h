@@ -178,6 +178,44 @@ int gp5cu_stepper_launches_per_step(const gp5cu_stepper *st);
 int gp5cu_stepper_profile(gp5cu_stepper *st, void *dfield, int nrep, double *ms, int *kinds, int cap,
                           int *nlaunch);
 
+/* ---- batched independent ground-state solves ---------------------------------------------
+ * No reference counterpart (the reference runs one solve per process; its imaginary-time
+ * protocol is python/test/regressionTests/LHY_imaginary.py).  Many LHY droplet solves, each
+ * on its own cubic grid, box, atom number, coefficients and time step, advance together:
+ * solves of the same grid size share every kernel launch (one launch per pass covers all of
+ * them), the steps between convergence checks replay from one CUDA graph, and solves that
+ * reach the residual tolerance stop (their tiles return at once). */
+typedef struct gp5cu_batch gp5cu_batch;
+
+typedef struct gp5cu_solve_desc {
+    int n;          /* grid points per axis (n^3 grid); power of two in [32, 512] */
+    double L;       /* box [-L/2, L/2]^3 */
+    double N;       /* atom number: the state is renormalised to it every step */
+    double c3, c4;  /* H = -1/2 lap + (c3 n + c4 n^{3/2}) + V */
+    double omega;   /* isotropic harmonic trap V = omega^2 r^2 / 2 (0: none) */
+    double dt;      /* imaginary time step */
+} gp5cu_solve_desc;
+
+typedef struct gp5cu_solve_result {
+    int steps;        /* RK4 steps taken (0 if the initial state already met tol) */
+    int converged;    /* residual <= tol */
+    double residual;  /* ||H psi - mu psi|| / ||psi|| at the last check */
+    double energy, mu, norm;
+} gp5cu_solve_result;
+
+int gp5cu_batch_create(gp5cu_batch **out, int nsolves, const gp5cu_solve_desc *solves, int precision,
+                       int device);
+int gp5cu_batch_destroy(gp5cu_batch *b);
+/* Initial / current state of one solve, complex128 host data of n^3 elements. */
+int gp5cu_batch_set_state(gp5cu_batch *b, int solve, const double *host_c128);
+int gp5cu_batch_get_state(gp5cu_batch *b, int solve, double *host_c128);
+/* Imaginary-time RK4 of every solve until residual <= tol (checked every check_every steps)
+ * or max_steps; results[i] per solve.  Returns GP5_OK even if some solves did not converge. */
+int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps,
+                      gp5cu_solve_result *results);
+/* Kernel launches of the last gp5cu_batch_solve call. */
+long long gp5cu_batch_launches(const gp5cu_batch *b);
+
 /* ---- allocation-free norm ---------------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc when they need
  * a norm (their device memory belongs to another allocator, or the device is full): the same

@@ -1,0 +1,86 @@
+"""Batched independent droplet solves (gp5cu_batch_*) against single solves and the oracle."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import gp_oracle as o
+
+pytestmark = pytest.mark.gpu
+
+
+def droplet_start(n, L, N, seed):
+    geo = o.Geometry((n,) * 3, (-L / 2,) * 3, (L / 2,) * 3)
+    return geo, o.gaussian_with_noise(geo, 0.5 * N ** (1 / 3), 1e-3, seed=seed, N=N, phase_noise=True)
+
+
+SOLVES = [
+    dict(n=32, L=12.0, N=20.0, c3=-3.0, c4=2.5, omega=0.0, dt=0.004),
+    dict(n=64, L=20.0, N=200.0, c3=-2.9, c4=2.5, omega=0.1, dt=0.003),
+    dict(n=32, L=14.0, N=40.0, c3=-3.1, c4=2.5, omega=0.05, dt=0.005),
+    dict(n=64, L=24.0, N=500.0, c3=-3.2, c4=2.5, omega=0.0, dt=0.004),
+    dict(n=32, L=10.0, N=25.0, c3=-2.8, c4=2.5, omega=0.0, dt=0.003),
+]
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_batch_matches_single_solves(prec):
+    from gp5_b200 import _abi as abi
+    b = abi.Batch(SOLVES, precision=prec)
+    starts = []
+    for k, sd in enumerate(SOLVES):
+        geo, psi = droplet_start(sd["n"], sd["L"], sd["N"], 100 + k)
+        starts.append((geo, psi))
+        b.set_state(k, psi)
+    res = b.solve(tol=1e-30, check_every=10, max_steps=30)
+    assert all(r["steps"] == 30 and not r["converged"] for r in res)
+    for k, sd in enumerate(SOLVES):
+        geo, psi = starts[k]
+        p = abi.Plan(geo.shape, geo.left, geo.right, precision=prec)
+        f = abi.Functional(p, abi.GP5_FUNC_LHY, c3=sd["c3"], c4=sd["c4"],
+                           omegas=[(sd["omega"],) * 3] if sd["omega"] > 0 else None)
+        st = abi.Stepper(f, sd["dt"])
+        st.set_renormalization([sd["N"]])
+        a = p.field(psi)
+        for _ in range(3):
+            st.advance(a, 10)
+        single = a.download()
+        batched = b.get_state(k)
+        assert np.array_equal(single, batched), k
+        ob = f.observables(a)
+        assert abs(ob["residual"] - res[k]["residual"]) <= 1e-12 * max(ob["residual"], 1e-300) + 1e-300
+        assert abs(ob["energy"] - res[k]["energy"]) <= 1e-12 * abs(ob["energy"])
+
+
+def test_batch_vs_oracle():
+    from gp5_b200 import _abi as abi
+    sd = SOLVES[2]
+    geo, psi = droplet_start(sd["n"], sd["L"], sd["N"], 7)
+    b = abi.Batch([sd])
+    b.set_state(0, psi)
+    b.solve(tol=1e-30, check_every=5, max_steps=20)
+    V = o.harmonic_potential(geo, [(sd["omega"],) * 3])
+    st = o.Stepper(o.Functional("lhy", c3=sd["c3"], c4=sd["c4"], V=V), geo, sd["dt"], normalizations=[sd["N"]])
+    ref = st.advance(psi.copy(), 20)
+    got = b.get_state(0)
+    assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-12
+
+
+def test_batch_converges_to_residual():
+    from gp5_b200 import _abi as abi
+    solves = [dict(n=32, L=4 * 20 ** (1 / 3), N=20.0, c3=-3.0, c4=2.5, omega=0.0, dt=0.01),
+              dict(n=32, L=4 * 30 ** (1 / 3), N=30.0, c3=-3.1, c4=2.5, omega=0.0, dt=0.01)]
+    b = abi.Batch(solves)
+    for k, sd in enumerate(solves):
+        geo, psi = droplet_start(sd["n"], sd["L"], sd["N"], 11 + k)
+        b.set_state(k, psi)
+    res = b.solve(tol=1e-8, check_every=100, max_steps=200000)
+    for k, (r, sd) in enumerate(zip(res, solves)):
+        assert r["converged"], r
+        assert r["residual"] <= 1e-8
+        geo = o.Geometry((sd["n"],) * 3, (-sd["L"] / 2,) * 3, (sd["L"] / 2,) * 3)
+        ob = o.observables(o.Functional("lhy", c3=sd["c3"]), b.get_state(k), geo)
+        assert abs(ob["E"] - r["energy"]) <= 1e-10 * abs(ob["E"])
+        assert abs(ob["mu"] - r["mu"]) <= 1e-10 * abs(ob["mu"])
+        assert abs(ob["norm"] - sd["N"]) <= 1e-9 * sd["N"]
+        assert math.isclose(ob["residual"], r["residual"], rel_tol=1e-6)
