@@ -126,3 +126,20 @@ def test_lhy_mu_protocol_near_reference_golden():
     mu, blocks, _ = o.lhy_mu_protocol()
     assert abs(mu - (-0.3837299937094331)) < 1e-4
     assert abs(mu - (-0.3836663826072363)) < 1e-12
+
+
+def test_rk4_imaginary_stability_bound_on_corner_modes():
+    """Renormalised imaginary-time RK4 blows up once dt passes 2.785 / (1.5 (pi/dx)^2)
+    ~ 0.188 dx^2: white noise excites the cube-corner modes K^2 = 3 (pi/dx)^2, whose RK4
+    amplification leaves [-1, 1].  (The batched ground-state runs use 0.15 dx^2.)"""
+    geo = o.Geometry((16, 16, 16), (-4,) * 3, (4,) * 3)
+    psi = o.gaussian_with_noise(geo, 1.5, 1e-3, seed=4, N=20.0, phase_noise=True)
+    dx = geo.space_step(0)
+    f = o.Functional("lhy")
+    grow = []
+    for fac in (0.15, 0.2):
+        st = o.Stepper(f, geo, fac * dx * dx, normalizations=[20.0])
+        e0 = o.observables(f, psi, geo)["ekin"]
+        e1 = o.observables(f, st.advance(psi.copy(), 300), geo)["ekin"]
+        grow.append(e1 / e0)
+    assert grow[0] < 1.0 and grow[1] > 3.0
