@@ -131,6 +131,16 @@ def lib():
         "gp5cu_batch_get_state": (i, [vp, i, vp]),
         "gp5cu_batch_solve": (i, [vp, d, i, i, C.POINTER(SolveResult)]),
         "gp5cu_batch_launches": (C.c_longlong, [vp]),
+        "gp5cu_mlp_create": (i, [pp, i, C.c_ulonglong]),
+        "gp5cu_mlp_destroy": (i, [vp]),
+        "gp5cu_mlp_num_params": (C.c_longlong, [vp]),
+        "gp5cu_mlp_get_params": (i, [vp, vp]),
+        "gp5cu_mlp_set_params": (i, [vp, vp]),
+        "gp5cu_mlp_forward": (i, [vp, vp, i, vp]),
+        "gp5cu_mlp_gradients": (i, [vp, vp, vp, i, vp, C.POINTER(d)]),
+        "gp5cu_mlp_train": (i, [vp, vp, vp, i, i, i, C.c_float, C.c_ulonglong, vp]),
+        "gp5cu_gemm_bf16": (i, [vp, C.c_longlong, C.c_longlong, vp, C.c_longlong, C.c_longlong, vp,
+                                C.c_longlong, i, i, i, vp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(L, name)
@@ -429,3 +439,75 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def bf16_round(a: np.ndarray) -> np.ndarray:
+    """float32 values rounded to the nearest BF16 (ties to even), returned as float32."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+class Mlp:
+    """The warm-start MLP (gp5cu_mlp_*): 3 -> 256 -> 256 -> 256 -> 64, GELU hidden layers."""
+
+    IN, HIDDEN, OUT = 3, 256, 64
+    SHAPES = [(256, 3), (256, 256), (256, 256), (64, 256)]
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = C.c_void_p()
+        check(lib().gp5cu_mlp_create(C.byref(h), device, int(seed)))
+        self.h = h
+        self.nparam = int(lib().gp5cu_mlp_num_params(self.h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.nparam, dtype=np.float32)
+        check(lib().gp5cu_mlp_get_params(self.h, C.c_void_p(_ptr(out))))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        assert a.size == self.nparam
+        check(lib().gp5cu_mlp_set_params(self.h, C.c_void_p(_ptr(a))))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.IN)
+        y = np.empty((x.shape[0], self.OUT), dtype=np.float32)
+        check(lib().gp5cu_mlp_forward(self.h, C.c_void_p(_ptr(x)), x.shape[0], C.c_void_p(_ptr(y))))
+        return y
+
+    def gradients(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.IN)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, self.OUT)
+        g = np.empty(self.nparam, dtype=np.float32)
+        loss = C.c_double()
+        check(lib().gp5cu_mlp_gradients(self.h, C.c_void_p(_ptr(x)), C.c_void_p(_ptr(t)), x.shape[0],
+                                        C.c_void_p(_ptr(g)), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int, batch: int = 256, lr: float = 1e-3,
+              seed: int = 0) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, self.IN)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, self.OUT)
+        hist = np.empty(epochs, dtype=np.float32)
+        check(lib().gp5cu_mlp_train(self.h, C.c_void_p(_ptr(x)), C.c_void_p(_ptr(t)), x.shape[0], int(epochs),
+                                    int(batch), float(lr), int(seed), C.c_void_p(_ptr(hist))))
+        return hist
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gp5cu_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gemm_bf16(A_dev: int, sam: int, sak: int, B_dev: int, sbn: int, sbk: int, C_dev: int, ldc: int,
+              M: int, N: int, K: int, stream: int = 0) -> None:
+    """C = A B^T on device pointers (BF16 operands, FP32 result), see gp5cu_gemm_bf16."""
+    check(lib().gp5cu_gemm_bf16(C.c_void_p(A_dev), sam, sak, C.c_void_p(B_dev), sbn, sbk, C.c_void_p(C_dev), ldc,
+                                M, N, K, C.c_void_p(stream)))

@@ -216,6 +216,36 @@ int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps
 /* Kernel launches of the last gp5cu_batch_solve call. */
 long long gp5cu_batch_launches(const gp5cu_batch *b);
 
+/* ---- learned warm start ------------------------------------------------------------------
+ * No counterpart in the reference, which starts every solve from a Gaussian
+ * (python/test/regressionTests/LHY_imaginary.py:14).  A 3 -> 256 -> 256 -> 256 -> 64 MLP with
+ * GELU hidden layers maps solve parameters to radial samples of the ground state.  Its GEMMs
+ * are tcgen05 tensor-core kernels with BF16 operands and FP32 accumulation; parameters are
+ * kept in FP32 (Adam's master copy) and used as BF16.
+ * Parameter vector layout (gp5cu_mlp_num_params floats): for each layer l, W_l row-major
+ * [fan_out][fan_in], then b_l [fan_out].  Inputs x are [B][3] and outputs/targets [B][64],
+ * row-major FP32 host arrays. */
+typedef struct gp5cu_mlp gp5cu_mlp;
+int gp5cu_mlp_create(gp5cu_mlp **out, int device, unsigned long long seed);
+int gp5cu_mlp_destroy(gp5cu_mlp *net);
+long long gp5cu_mlp_num_params(const gp5cu_mlp *net);
+int gp5cu_mlp_get_params(gp5cu_mlp *net, float *host);
+int gp5cu_mlp_set_params(gp5cu_mlp *net, const float *host);
+/* inference of B samples: y[B][64] */
+int gp5cu_mlp_forward(gp5cu_mlp *net, const float *x, int B, float *y);
+/* gradient of the loss sum((y - t)^2) / (B * 64) with respect to every parameter (same layout
+ * as the parameter vector) and the loss itself */
+int gp5cu_mlp_gradients(gp5cu_mlp *net, const float *x, const float *t, int B, float *grad, double *loss);
+/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) over `epochs` seeded shuffles of the `count`
+ * samples in mini-batches of `batch` (a trailing partial batch is skipped);
+ * loss_history[epoch] (may be NULL) receives each epoch's mean loss. */
+int gp5cu_mlp_train(gp5cu_mlp *net, const float *x, const float *t, int count, int epochs, int batch, float lr,
+                    unsigned long long seed, float *loss_history);
+/* C[m*ldc + n] = sum_k A(m,k) B(n,k), A(m,k) = A[m*sam + k*sak], B(n,k) = B[n*sbn + k*sbk]:
+ * BF16 device operands, FP32 device result, on `stream` (cudaStream_t or NULL; synchronised) */
+int gp5cu_gemm_bf16(const void *A, long long sam, long long sak, const void *B, long long sbn, long long sbk,
+                    float *C, long long ldc, int M, int N, int K, void *stream);
+
 /* ---- allocation-free norm ---------------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc when they need
  * a norm (their device memory belongs to another allocator, or the device is full): the same
