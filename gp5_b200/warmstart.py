@@ -21,6 +21,7 @@ import numpy as np
 from . import _abi
 
 N_SAMPLES = 64
+DEFAULT_WEIGHTS = __import__("os").path.join(__import__("os").path.dirname(__file__), "data", "warmstart_mlp.npz")
 OMEGAS = (0.0, 0.05, 0.1)
 C4 = 2.5
 
@@ -119,21 +120,97 @@ def radial_samples(psi: np.ndarray, N: float) -> np.ndarray:
     return acc / 6.0
 
 
+_BASIS = None
+
+
+def _basis():
+    """Cubic-spline basis on the normalised sample radii u_j = j/63 (zero slope at u = 0,
+    not-a-knot at u = 1): f(u) = B(u) @ samples."""
+    global _BASIS
+    if _BASIS is None:
+        from scipy.interpolate import CubicSpline
+
+        u = np.linspace(0.0, 1.0, N_SAMPLES)
+        _BASIS = CubicSpline(u, np.eye(N_SAMPLES), bc_type=((1, np.zeros(N_SAMPLES)), "not-a-knot"))
+    return _BASIS
+
+
+def _profile_matrix(d: np.ndarray, R: float, kappa: float) -> np.ndarray:
+    """(len(d), 64) matrix M with f(d) = M @ samples: the spline up to R, and beyond R a
+    screened-Coulomb (Yukawa) tail f(R) (R/d) exp(-kappa (d - R))."""
+    d = np.asarray(d, dtype=np.float64)
+    inside = d <= R
+    M = np.where(inside[:, None], _basis()(np.minimum(d, R) / R), 0.0)
+    do = np.maximum(d, R)
+    M[:, -1] += np.where(inside, 0.0, (R / do) * np.exp(-kappa * (do - R)))
+    return M
+
+
+def _tail_kappa(f: np.ndarray, r: np.ndarray) -> float:
+    """Decay rate of r f(r) over samples 54..60 (log-linear least squares), clipped to [0.1, 5]."""
+    sl = slice(-10, -3)
+    y = np.log(np.maximum(r[sl] * np.abs(f[sl]), 1e-300))
+    return float(np.clip(-np.polyfit(r[sl], y, 1)[0], 0.1, 5.0))
+
+
+_AXIS_IMAGES = [(a, b, c) for a in range(-2, 3) for b in range(-2, 3) for c in range(-2, 3)]
+_GRID_IMAGES = [(a, b, c) for a in range(-1, 2) for b in range(-1, 2) for c in range(-1, 2)]
+
+
+def free_profile(samples: np.ndarray, N: float, iters: int = 4):
+    """The isolated-droplet profile f whose periodic image sum sum_m f(|x - m L|) has the given
+    samples along the axes; returns (f samples at radii(N), tail decay rate kappa).
+
+    A ground state in the periodic box [-L/2, L/2]^3 is, where its density is small, a solution
+    of the linear equation (-1/2 lap - mu) psi = 0, so its tail is a lattice sum of screened
+    Coulomb tails, one per periodic image of the droplet.  Along the axis the image terms are
+    a small correction, so the 64 x 64 system (spline inside R = L/2, Yukawa tail outside,
+    images up to two boxes away) is diagonally dominant; kappa is re-estimated from the
+    solution's own tail at each of the `iters` passes."""
+    a = np.maximum(np.asarray(samples, dtype=np.float64), 0.0)
+    r = radii(N)
+    R, L = r[-1], box_length(N)
+    f = a.copy()
+    kappa = _tail_kappa(a, r)
+    for _ in range(iters):
+        A = np.zeros((N_SAMPLES, N_SAMPLES))
+        for m in _AXIS_IMAGES:
+            d = np.sqrt((r - m[0] * L) ** 2 + (m[1] * L) ** 2 + (m[2] * L) ** 2)
+            A += _profile_matrix(d, R, kappa)
+        f = np.linalg.solve(A, a)
+        kappa = _tail_kappa(f, r)
+    return f, kappa
+
+
 def profile_start(samples: np.ndarray, N: float, n: int, seed: Optional[int] = None,
                   amp: float = 1e-3) -> np.ndarray:
-    """Radial samples interpolated onto the n^3 grid (cubic spline with zero slope at r = 0;
-    beyond the last radius the last sample), clipped at zero, phase noise as for the Gaussian,
-    normalised to N; complex128 (n, n, n), Fortran order."""
-    from scipy.interpolate import CubicSpline
+    """Radial samples of a droplet in the periodic box, placed on the n^3 grid.
 
-    s = np.maximum(np.asarray(samples, dtype=np.float64), 0.0)
+    The samples (|psi| along the axes, as radial_samples returns) are turned into the isolated
+    profile f (free_profile), and the field is the image sum sum_m f(|x - m L|) over the 27
+    nearest periodic images, clipped at zero, with phase noise as for the Gaussian and
+    normalised to N; complex128 (n, n, n), Fortran order.  A purely radial placement would
+    miss the cubic (image-induced) shape of a small droplet's tail, which imaginary time then
+    removes only at the slow rate |mu|."""
+    f, kappa = free_profile(samples, N)
     r = radii(N)
-    spl = CubicSpline(r, s, bc_type=((1, 0.0), "not-a-knot"))
-    L = box_length(N)
+    R, L = r[-1], box_length(N)
     x = axis(n, L)
-    R = np.sqrt(x[:, None, None] ** 2 + x[None, :, None] ** 2 + x[None, None, :] ** 2)
-    prof = np.where(R <= r[-1], spl(np.minimum(R, r[-1])), s[-1])
-    psi = np.maximum(prof, 0.0).astype(np.complex128)
+    h = n // 2
+    xp = x[h:]  # the field is symmetric under each x_i -> -x_i: build one octant
+    dmax = math.sqrt(3.0) * (xp[-1] + L)
+    tab_d = np.linspace(0.0, dmax, 400001)
+    tab_f = _profile_matrix(tab_d, R, kappa) @ f
+    octant = np.zeros((n - h,) * 3)
+    for m in _GRID_IMAGES:
+        d = np.sqrt((xp[:, None, None] - m[0] * L) ** 2 + (xp[None, :, None] - m[1] * L) ** 2
+                    + (xp[None, None, :] - m[2] * L) ** 2)
+        octant += np.interp(d, tab_d, tab_f)
+    if n % 2:
+        raise ValueError("profile_start needs an even grid")
+    line = np.concatenate([np.arange(h - 1, -1, -1), np.arange(h)])  # x_i -> |x_i| index
+    psi = octant[np.ix_(line, line, line)]
+    psi = np.maximum(psi, 0.0).astype(np.complex128)
     psi = _phase_noise(psi, seed, amp)
     return np.asfortranarray(_normalise(psi, N, L / n))
 
@@ -183,7 +260,7 @@ class WarmStart:
         np.savez_compressed(path, params=self.get_params())
 
     @classmethod
-    def load(cls, path: str, device: int = 0) -> "WarmStart":
+    def load(cls, path: str = DEFAULT_WEIGHTS, device: int = 0) -> "WarmStart":
         with np.load(path) as z:
             return cls(device=device, params=z["params"])
 
@@ -194,25 +271,184 @@ class WarmStart:
 # ---- data from the batched solver -----------------------------------------------------------
 def solve_ground_states(params: Sequence[dict], grid, tol: float, chunk: int = 512,
                         check_every: int = 100, max_steps: int = 400000, precision: int = _abi.GP5_C128,
-                        starts=None, device: int = 0, seed: int = 0, keep=None):
+                        starts=None, device: int = 0, seed: int = 0, keep=None,
+                        caps: Sequence[int] = (1000, 3000, 10000, 30000, 100000, 400000), progress=None):
     """Solves every parameter set with the batched solver from a Gaussian (or
     starts(p, n, index)) on grid(p) (an int or a function of p); returns (states, results)
-    lists, each state passed through keep(p, psi) when keep is given."""
-    states, results = [], []
-    for c0 in range(0, len(params), chunk):
-        part = params[c0:c0 + chunk]
-        descs = [solve_desc(p, grid(p) if callable(grid) else int(grid)) for p in part]
-        b = _abi.Batch(descs, precision=precision, device=device)
-        try:
-            for k, (p, d) in enumerate(zip(part, descs)):
-                psi = (starts(p, d["n"], c0 + k) if starts is not None
-                       else gaussian_start(p["N"], d["n"], seed + c0 + k))
-                b.set_state(k, psi)
-            res = b.solve(tol=tol, check_every=check_every, max_steps=max_steps)
-            for k, p in enumerate(part):
-                psi = b.get_state(k)[..., 0]
-                states.append(keep(p, psi) if keep is not None else psi)
-            results.extend(res)
-        finally:
-            b.close()
+    lists in the order of params, each state passed through keep(p, psi) when keep is given.
+
+    A converged solve stops costing arithmetic but still takes part in every launch of its
+    batch, so the solves run in rounds: round j advances every unconverged solve up to caps[j]
+    steps in total, and the next round re-batches only those still above tol (from their
+    current states; the trajectory is the same as one uninterrupted run, since the RK4 step
+    carries no state besides psi).  results[i]["steps"] counts all rounds; progress(cap, n)
+    is called before each round with the number of solves it advances."""
+    count = len(params)
+    gridof = (lambda p: grid(p)) if callable(grid) else (lambda p: int(grid))
+    descs = [solve_desc(p, gridof(p)) for p in params]
+    done_steps = [0] * count
+    current = {}
+    states, results = [None] * count, [None] * count
+    pending = list(range(count))
+    caps = sorted({min(int(c), max_steps) for c in caps} | {max_steps})
+    for cap in caps:
+        if not pending:
+            break
+        if progress is not None:
+            progress(cap, len(pending))
+        still = []
+        for c0 in range(0, len(pending), chunk):
+            part = pending[c0:c0 + chunk]
+            b = _abi.Batch([descs[i] for i in part], precision=precision, device=device)
+            try:
+                for k, i in enumerate(part):
+                    if i in current:
+                        psi = current.pop(i)
+                    elif starts is not None:
+                        psi = starts(params[i], descs[i]["n"], i)
+                    else:
+                        psi = gaussian_start(params[i]["N"], descs[i]["n"], seed + i)
+                    b.set_state(k, psi)
+                budget = cap - max(done_steps[i] for i in part)
+                res = b.solve(tol=tol, check_every=check_every, max_steps=max(budget, check_every))
+                for k, i in enumerate(part):
+                    done_steps[i] += res[k]["steps"]
+                    r = dict(res[k])
+                    r["steps"] = done_steps[i]
+                    psi = b.get_state(k)[..., 0]
+                    if r["converged"] or cap >= max_steps:
+                        results[i] = r
+                        states[i] = keep(params[i], psi) if keep is not None else psi
+                    else:
+                        current[i] = np.asfortranarray(psi)
+                        still.append(i)
+            finally:
+                b.close()
+        pending = still
     return states, results
+
+
+# ---- training and evaluation ---------------------------------------------------------------
+TRAIN_SEED, TEST_SEED = 1, 2
+
+
+def training_grid(p: dict) -> int:
+    """32^3 where it gives a spacing of at most 0.5 (N <= 64), else 64^3."""
+    return smallest_grid(p["N"], (32, 64), 0.5)
+
+
+def make_training_set(count: int = 4096, seed: int = TRAIN_SEED, grid=training_grid, tol: float = 1e-7,
+                      chunk: int = 1024, device: int = 0):
+    """Ground states of `count` seeded parameter sets (batched imaginary-time RK4 in complex128
+    from the noise-free Gaussian, to residual tol, on grid(p)^3); returns (params, radial
+    samples [count][64], solver results)."""
+    params = sample_params(count, seed)
+    keep = lambda p, psi: radial_samples(psi, p["N"])
+    import sys
+    import time
+
+    t0 = time.time()
+    report = lambda cap, k: print(f"[{time.time() - t0:7.1f} s] round to {cap} steps: {k} solves",
+                                  file=sys.stderr, flush=True)
+    samples, results = solve_ground_states(params, grid, tol=tol, chunk=chunk, device=device, keep=keep,
+                                           progress=report,
+                                           starts=lambda p, n, k: gaussian_start(p["N"], n, None))
+    return params, np.asarray(samples), results
+
+
+def evaluate(model: "WarmStart", count: int = 64, seed: int = TEST_SEED, n: int = 128, tol: float = 1e-8,
+             check_every: int = 100, device: int = 0) -> dict:
+    """Steps to `tol` from the Gaussian and from the network's start for `count` unseen seeded
+    parameter sets on n^3 grids (complex128, both starts noise-free), with the converged
+    energies and the network's profile error against the converged states."""
+    import sys
+    import time
+
+    params = sample_params(count, seed)
+    pred = model.predict(params)
+    keep = lambda p, psi: radial_samples(psi, p["N"])
+    t0 = time.time()
+    report = lambda cap, k: print(f"[{time.time() - t0:7.1f} s] round to {cap} steps: {k} solves",
+                                  file=sys.stderr, flush=True)
+    sg, rg = solve_ground_states(params, n, tol=tol, chunk=count, check_every=check_every, device=device,
+                                 keep=keep, progress=report,
+                                 starts=lambda p, m, k: gaussian_start(p["N"], m, None))
+    sw, rw = solve_ground_states(params, n, tol=tol, chunk=count, check_every=check_every, device=device,
+                                 keep=keep, progress=report,
+                                 starts=lambda p, m, k: profile_start(pred[k], p["N"], m, None))
+    sg = np.asarray(sg)
+    steps_g = np.array([r["steps"] for r in rg])
+    steps_w = np.array([r["steps"] for r in rw])
+    Eg = np.array([r["energy"] for r in rg])
+    Ew = np.array([r["energy"] for r in rw])
+    peak = np.max(np.abs(sg), axis=1)
+    return dict(
+        count=count, seed=seed, grid=n, tol=tol, check_every=check_every,
+        params=params,
+        steps_gaussian=steps_g.tolist(), steps_warm=steps_w.tolist(),
+        converged_gaussian=[bool(r["converged"]) for r in rg], converged_warm=[bool(r["converged"]) for r in rw],
+        energy_gaussian=Eg.tolist(), energy_warm=Ew.tolist(),
+        total_steps_gaussian=int(steps_g.sum()), total_steps_warm=int(steps_w.sum()),
+        step_ratio_total=float(steps_g.sum() / max(steps_w.sum(), 1)),
+        step_ratio_median=float(np.median(steps_g / np.maximum(steps_w, 1))),
+        max_rel_energy_diff=float(np.max(np.abs(Ew - Eg) / np.abs(Eg))),
+        profile_rms_error=float(np.sqrt(np.mean((pred - sg) ** 2))),
+        profile_max_rel_error=float(np.max(np.abs(pred - sg) / peak[:, None])),
+    )
+
+
+def main(argv=None):
+    import argparse
+    import json
+    import os
+    import time
+
+    ap = argparse.ArgumentParser(description="Train or evaluate the droplet warm-start network.")
+    ap.add_argument("--train", metavar="OUT_NPZ", help="generate the training set, train, save weights")
+    ap.add_argument("--evaluate", metavar="MODEL_NPZ", help="evaluate saved weights on unseen droplets")
+    ap.add_argument("--report", metavar="JSON", help="where --evaluate writes its report")
+    ap.add_argument("--count", type=int, default=4096)
+    ap.add_argument("--epochs", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--decay-every", type=int, default=800)
+    ap.add_argument("--data", metavar="NPZ", help="reuse (or save) the training set here")
+    ap.add_argument("--test-count", type=int, default=64)
+    ap.add_argument("--test-grid", type=int, default=128)
+    a = ap.parse_args(argv)
+    if a.train:
+        t0 = time.time()
+        if a.data and os.path.exists(a.data):
+            z = np.load(a.data)
+            params = [dict(N=float(r[0]), c3=float(r[1]), omega=float(r[2])) for r in z["params"]]
+            samples, steps = z["samples"].astype(np.float64), z["steps"]
+        else:
+            params, samples, results = make_training_set(a.count)
+            steps = np.array([r["steps"] for r in results])
+            if a.data:
+                table = np.array([[p["N"], p["c3"], p["omega"]] for p in params])
+                np.savez_compressed(a.data, params=table, samples=samples.astype(np.float32),
+                                    steps=steps.astype(np.int32))
+        t1 = time.time()
+        model = WarmStart(seed=0)
+        hist = model.train(params, samples, a.epochs, a.batch, a.lr, seed=0, lr_decay_every=a.decay_every)
+        t2 = time.time()
+        model.save(a.train)
+        pred = model.predict(params)
+        print(json.dumps(dict(count=len(params), data_seconds=round(t1 - t0, 1), train_seconds=round(t2 - t1, 1),
+                              solver_steps_mean=float(np.mean(steps)), loss_first=float(hist[0]),
+                              loss_last=float(hist[-1]),
+                              train_rms=float(np.sqrt(np.mean((pred - samples) ** 2))))))
+    if a.evaluate:
+        model = WarmStart.load(a.evaluate)
+        t0 = time.time()
+        rep = evaluate(model, a.test_count, n=a.test_grid)
+        rep["seconds"] = round(time.time() - t0, 1)
+        if a.report:
+            with open(a.report, "w") as fh:
+                json.dump(rep, fh, indent=1)
+        print(json.dumps({k: v for k, v in rep.items() if not isinstance(v, list)}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,109 @@
+"""Host-side logic of the warm start (no GPU): re-batching of unconverged solves and the
+periodic image-sum placement of radial samples."""
+import math
+
+import numpy as np
+
+from gp5_b200 import warmstart as ws
+
+
+class FakeBatch:
+    """Stands in for _abi.Batch: solve i converges after need[i] steps in total."""
+    need = {}
+    created = []
+
+    def __init__(self, descs, precision=0, device=0):
+        self.descs = descs
+        self.states = [None] * len(descs)
+        FakeBatch.created.append(len(descs))
+
+    def set_state(self, k, psi):
+        self.states[k] = np.array(psi, copy=True)
+
+    def solve(self, tol, check_every, max_steps):
+        out = []
+        for k, d in enumerate(self.descs):
+            key = d["N"]
+            done = int(self.states[k].flat[0].real)
+            left = FakeBatch.need[key] - done
+            steps = min(max(left, 0), max_steps)
+            steps = int(math.ceil(steps / check_every) * check_every) if steps < max_steps else max_steps
+            self.states[k].flat[0] = done + steps
+            conv = done + steps >= FakeBatch.need[key]
+            out.append(dict(steps=steps, converged=int(conv), residual=0.0 if conv else 1.0,
+                            energy=-key, mu=-1.0, norm=key))
+        return out
+
+    def get_state(self, k):
+        return self.states[k][..., None]
+
+    def close(self):
+        pass
+
+
+def test_rebatching_counts_steps_and_keeps_order(monkeypatch):
+    params = [dict(N=float(20 + k), c3=-3.0, omega=0.0) for k in range(7)]
+    FakeBatch.need = {p["N"]: s for p, s in zip(params, [300, 5000, 900, 45000, 100, 2500, 12000])}
+    FakeBatch.created = []
+    monkeypatch.setattr(ws._abi, "Batch", FakeBatch)
+    starts = lambda p, n, i: np.zeros((4, 4, 4), complex)
+    states, res = ws.solve_ground_states(params, 4, tol=1e-8, chunk=3, starts=starts, check_every=100,
+                                         caps=(1000, 3000, 10000, 30000, 100000), max_steps=100000)
+    assert [r["steps"] for r in res] == [300, 5000, 900, 45000, 100, 2500, 12000]
+    assert all(r["converged"] for r in res)
+    assert [r["energy"] for r in res] == [-p["N"] for p in params]
+    # round sizes: 7 solves (chunks 3,3,1), then 4 above 1000 steps, 3 above 3000, 2, 1
+    assert FakeBatch.created == [3, 3, 1, 3, 1, 3, 2, 1]
+
+
+def test_rebatching_reports_unconverged_at_max_steps(monkeypatch):
+    params = [dict(N=21.0, c3=-3.0, omega=0.0), dict(N=22.0, c3=-3.0, omega=0.0)]
+    FakeBatch.need = {21.0: 700, 22.0: 10 ** 9}
+    FakeBatch.created = []
+    monkeypatch.setattr(ws._abi, "Batch", FakeBatch)
+    starts = lambda p, n, i: np.zeros((4, 4, 4), complex)
+    _, res = ws.solve_ground_states(params, 4, tol=1e-8, starts=starts, caps=(1000,), max_steps=4000)
+    assert res[0]["steps"] == 700 and res[0]["converged"]
+    assert res[1]["steps"] == 4000 and not res[1]["converged"]
+
+
+def _periodic_droplet(N, n, kappa=0.7):
+    """sum over images of a smooth core with a screened-Coulomb tail (the shape of a small
+    droplet's ground state in the periodic box)."""
+    L = ws.box_length(N)
+    x = ws.axis(n, L)
+    R = ws.radii(N)[-1]
+    rc = 0.4 * R
+
+    def f(d):
+        core = np.exp(-(d / rc) ** 2)
+        tail = 0.02 * np.exp(-kappa * d) / np.maximum(d, 0.5) * (1 - np.exp(-(d / rc) ** 4))
+        return core + tail
+
+    out = np.zeros((n, n, n))
+    for a in (-1, 0, 1):
+        for b in (-1, 0, 1):
+            for c in (-1, 0, 1):
+                d = np.sqrt((x[:, None, None] - a * L) ** 2 + (x[None, :, None] - b * L) ** 2
+                            + (x[None, None, :] - c * L) ** 2)
+                out += f(d)
+    return out * math.sqrt(N / (np.sum(out ** 2) * (L / n) ** 3))
+
+
+def test_image_sum_placement_reproduces_periodic_droplet():
+    N, n = 40.0, 48
+    psi = _periodic_droplet(N, n)
+    S = ws.radial_samples(psi, N)
+    got = ws.profile_start(S, N, n)
+    err = np.max(np.abs(got - psi)) / np.max(psi)
+    # a purely radial placement misses the image-induced corner tails
+    r = ws.radii(N)
+    L = ws.box_length(N)
+    x = ws.axis(n, L)
+    Rg = np.sqrt(x[:, None, None] ** 2 + x[None, :, None] ** 2 + x[None, None, :] ** 2)
+    radial = np.interp(np.minimum(Rg, r[-1]), r, S)
+    radial = radial * math.sqrt(N / (np.sum(radial ** 2) * (L / n) ** 3))
+    err_radial = np.max(np.abs(radial - psi)) / np.max(psi)
+    assert err < 2e-3 and err < 0.2 * err_radial, (err, err_radial)
+    assert got.flags["F_CONTIGUOUS"] and got.dtype == np.complex128
+    assert abs(np.sum(np.abs(got) ** 2) * (L / n) ** 3 - N) < 1e-9 * N
