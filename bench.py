@@ -143,13 +143,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kind_name: str):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+def ncu_traffic(kind_name: str, dtype: str):
+    """Per-launch DRAM bytes (read + write) of a kernel kind from the committed ncu summary of
+    the same workload and precision, if one exists."""
     p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        v = d.get(kind_name)
+        v = d.get(dtype, {}).get(kind_name)
         if isinstance(v, dict):
             return v.get("bytes_per_launch_256cubed")
     return None
@@ -231,7 +232,7 @@ def run_ours(args, rank, world, local_rank):
     return results, launches
 
 
-def roofline(r):
+def roofline(r, dtype: str = "c128"):
     """Dominant kernel (largest share of a step) with its algorithmic bytes per launch."""
     prof = r["profile"]
     F = r["field_bytes"]
@@ -255,7 +256,7 @@ def roofline(r):
     peak, src = measured_peaks()
     achieved = b / (ms / 1e3) / 1e9
     name = KIND_NAMES.get(kind, str(kind))
-    traffic = ncu_traffic(name)
+    traffic = ncu_traffic(name, dtype)
     step_bytes = sum(bytes_per)
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "peak_source": src, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -415,8 +416,8 @@ def main():
             "data": "synthetic", "config": config,
             "fp32": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "dtype": "c64",
                      "speedup_vs_fp64": r32["value"] / r64["value"], "clocks": r32["clocks"],
-                     "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2))},
-            "e2e": r64["e2e"], "roofline": roofline(r64), "cpu_baseline": cpu,
+                     "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2), "c64")},
+            "e2e": r64["e2e"], "roofline": roofline(r64, "c128"), "cpu_baseline": cpu,
             "clocks": r64["clocks"], "gpu_launches": launches, "ground_states": gs,
             "launches_per_step": r64["launches_per_step"]}
     print(json.dumps(line))
