@@ -196,7 +196,7 @@ def run_ours(args, rank, world, local_rank):
         lps = st.launches_per_step
         launches += lps * args.steps + 1  # + the prologue transform of each advance call
         r = {"ms": ms, "ms_per_step": ms / args.steps, "value": world * sites * args.steps / (ms / 1e3),
-             "clocks": clk.summary(), "launches_per_step": lps}
+             "clocks": clk.summary(), "launches_per_step": lps, "tiles": plan.tiles()}
         # per-launch durations of one step (CUDA events between launches, same stream)
         prof = st.profile(f, nrep=3)
         r["profile"] = prof
@@ -418,7 +418,9 @@ def main():
                      "speedup_vs_fp64": r32["value"] / r64["value"], "clocks": r32["clocks"],
                      "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2), "c64")},
             "e2e": r64["e2e"], "roofline": roofline(r64, "c128"), "cpu_baseline": cpu,
-            "clocks": r64["clocks"], "gpu_launches": launches, "ground_states": gs,
+            "clocks": r64["clocks"], "gpu_launches": launches,
+            "autotune": {"passes": ["y_fwd", "y_inv", "z_fwd", "z_inv", "z_fwd_kinetic_inv"],
+                         "threads_per_cta": {"c128": r64["tiles"], "c64": r32["tiles"]}}, "ground_states": gs,
             "launches_per_step": r64["launches_per_step"]}
     print(json.dumps(line))
 

@@ -131,6 +131,9 @@ def lib():
         "gp5cu_batch_get_state": (i, [vp, i, vp]),
         "gp5cu_batch_solve": (i, [vp, d, i, i, C.POINTER(SolveResult)]),
         "gp5cu_batch_launches": (C.c_longlong, [vp]),
+        "gp5cu_plan_autotune": (i, [vp]),
+        "gp5cu_plan_get_tiles": (i, [vp, C.POINTER(C.c_int)]),
+        "gp5cu_plan_set_tiles": (i, [vp, C.POINTER(C.c_int)]),
         "gp5cu_mlp_create": (i, [pp, i, C.c_ulonglong]),
         "gp5cu_mlp_destroy": (i, [vp]),
         "gp5cu_mlp_num_params": (C.c_longlong, [vp]),
@@ -212,6 +215,19 @@ class Plan:
         out = C.c_double()
         check(lib().gp5cu_max_density(self.h, f.ptr, C.byref(out)))
         return out.value
+
+    def tiles(self):
+        """Threads per CTA of (y fwd, y inv, z fwd, z inv, z fwd*K^2*inv); 0 = default shape."""
+        t = (C.c_int * 5)()
+        check(lib().gp5cu_plan_get_tiles(self.h, t))
+        return list(t)
+
+    def set_tiles(self, threads) -> None:
+        t = (C.c_int * 5)(*[int(v) for v in threads])
+        check(lib().gp5cu_plan_set_tiles(self.h, t))
+
+    def autotune(self) -> None:
+        check(lib().gp5cu_plan_autotune(self.h))
 
     def synchronize(self) -> None:
         check(lib().gp5cu_plan_synchronize(self.h))

@@ -3,7 +3,9 @@
 // Host logic only; the kernels and their launch sequences live in launch_impl.cuh.  Every
 // entry point catches the library's internal errors and returns a status code; the message
 // is kept per thread for gp5cu_last_error().
+#include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -119,6 +121,14 @@ void build_axis_plan(gp5cu_plan *p, int d) {
     const int n = p->shape[d];
     ap.n = n;
     ap.reg = (n == 32 || n == 64 || n == 128 || n == 256 || n == 512);
+    switch (n) {
+        case 32: ap.reg_threads = RegCfgAll<32>::T; break;
+        case 64: ap.reg_threads = RegCfgAll<64>::T; break;
+        case 128: ap.reg_threads = RegCfgAll<128>::T; break;
+        case 256: ap.reg_threads = RegCfgAll<256>::T; break;
+        case 512: ap.reg_threads = RegCfgAll<512>::T; break;
+        default: ap.reg_threads = 0;
+    }
     if (!factorize(n, ap.sched))
         fail(GP5_ERR_UNSUPPORTED, "axis length " + std::to_string(n) + " has a prime factor > 61");
     ap.tw = p->prec == GP5_C128 ? upload_twiddles<double>(n) : upload_twiddles<float>(n);
@@ -199,6 +209,29 @@ static SolveParams geometry_params(const int shape[3], const double left[3], con
 }
 
 // A plan for nsolve independent solves of one grid (boxes may differ per solve).
+// Tile shapes chosen by the autotuner, per (device, shape, components, precision, solves).
+// GP5_AUTOTUNE=0 in the environment keeps the default shapes.
+static std::mutex g_tune_mu;
+static std::map<std::array<long long, 7>, std::array<int, 12>> g_tune_cache;
+
+void autotune_plan(gp5cu_plan *p, bool force) {
+    const char *env = std::getenv("GP5_AUTOTUNE");
+    if (!force && env && std::string(env) == "0") return;
+    const std::array<long long, 7> key{p->dev, p->shape[0], p->shape[1], p->shape[2], p->ncomp, p->prec, p->nsolve};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (!force && it != g_tune_cache.end()) {
+        std::memcpy(p->tile_threads, it->second.data(), sizeof(p->tile_threads));
+        return;
+    }
+    if (p->prec == GP5_C128) Launch<double>::autotune(p, 3);
+    else Launch<float>::autotune(p, 3);
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    std::array<int, 12> v{};
+    std::memcpy(v.data(), p->tile_threads, sizeof(p->tile_threads));
+    g_tune_cache[key] = v;
+}
+
 gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const double *const *rights, int nsolve,
                         int ncomp, int precision, int device) {
     require(ncomp == 1 || ncomp == 2, "ncomp must be 1 or 2");
@@ -259,6 +292,7 @@ gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const do
         check_cuda(cudaMalloc(&p->dmax, sizeof(unsigned long long)), "cudaMalloc dmax");
         set_scalars(p->stream, p->ds, nsolve);
         check_cuda(cudaStreamSynchronize(p->stream), "sync");
+        autotune_plan(p, false);
     } catch (...) {
         gp5cu_plan_destroy(p);
         throw;
@@ -310,6 +344,34 @@ int gp5cu_plan_destroy(gp5cu_plan *p) {
     if (p->own_stream) cudaStreamDestroy(p->own_stream);
     delete p;
     return GP5_OK;
+}
+
+int gp5cu_plan_autotune(gp5cu_plan *p) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    use_device(p);
+    autotune_plan(p, true);
+    GP5_CATCH
+}
+
+int gp5cu_plan_get_tiles(const gp5cu_plan *p, int threads[5]) {
+    GP5_TRY
+    require(p != nullptr && threads != nullptr, "NULL argument");
+    for (int q = 0; q < kTunedPasses; q++) threads[q] = p->tile_threads[kTunedAxis[q]][kTunedMode[q]];
+    GP5_CATCH
+}
+
+int gp5cu_plan_set_tiles(gp5cu_plan *p, const int threads[5]) {
+    GP5_TRY
+    require(p != nullptr && threads != nullptr, "NULL argument");
+    for (int q = 0; q < kTunedPasses; q++) {
+        const int t = threads[q];
+        require(t == 0 || t == 128 || t == 256 || t == 512, "tile threads must be 0, 128, 256 or 512");
+        const AxisPlan &ap = p->ax[kTunedAxis[q]];
+        require(t == 0 || (ap.reg && t % ap.reg_threads == 0), "tile threads do not fit this axis");
+    }
+    for (int q = 0; q < kTunedPasses; q++) p->tile_threads[kTunedAxis[q]][kTunedMode[q]] = threads[q];
+    GP5_CATCH
 }
 
 int gp5cu_plan_set_stream(gp5cu_plan *p, void *stream) {

@@ -64,19 +64,36 @@ template <class K> inline void ensure_smem(K kernel, size_t bytes, int dev) {
     if (bytes > 48 * 1024) smem_opt_in((const void *)kernel, bytes, dev);
 }
 
-template <typename Real, int N, bool CONTIG, int MODE, class Op>
-void launch_reg(gp5cu_plan *p, int axis, const Op &op) {
+template <typename Real, int N, bool CONTIG, int MODE, class Op, int TH>
+void launch_reg_th(gp5cu_plan *p, int axis, const Op &op) {
     using V = cpx<Real>;
-    constexpr int LINES = RegTile<Real, N, CONTIG, MODE>::LINES, THREADS = RegTile<Real, N, CONTIG, MODE>::THREADS;
+    constexpr int LINES = RegTile<Real, N, CONTIG, MODE, TH>::LINES, THREADS = RegTile<Real, N, CONTIG, MODE, TH>::THREADS;
     long long tiles = 0;
     TileGeom g = make_geom(p, axis, LINES, true, &tiles);
     const size_t smem = CONTIG ? (size_t)LINES * LayContig<N>::LD * sizeof(V) : (size_t)LINES * N * sizeof(V);
-    auto kern = k_axis_reg<Real, N, CONTIG, MODE, Op>;
+    auto kern = k_axis_reg<Real, N, CONTIG, MODE, Op, TH>;
     ensure_smem(kern, smem, p->dev);
     if (p->dry) return;
     kern<<<(unsigned)tiles, THREADS, smem, p->stream>>>(g, op, (const V *)p->ax[axis].tw, red_slot(p));
     check_cuda(cudaGetLastError(), "k_axis_reg launch");
     if (p->prof) p->prof->record(p->stream, axis * 10 + MODE);
+}
+
+// Tile shapes of the strided (y/z) passes: the plan's autotuned threads per CTA (0: the
+// default rule of RegTile).  These passes carry no reductions, so the choice does not change
+// any result bit.
+template <typename Real, int N, bool CONTIG, int MODE, class Op>
+void launch_reg(gp5cu_plan *p, int axis, const Op &op) {
+    if constexpr (!CONTIG && (MODE == MODE_FWD || MODE == MODE_INV || MODE == MODE_FWD_MID_INV)) {
+        constexpr int T = RegCfgAll<N>::T, DEF = RegTile<Real, N, CONTIG, MODE, 0>::THREADS;
+        switch (p->tile_threads[axis][MODE]) {
+            case 128: if constexpr (128 % T == 0 && DEF != 128) { launch_reg_th<Real, N, CONTIG, MODE, Op, 128>(p, axis, op); return; } break;
+            case 256: if constexpr (256 % T == 0 && DEF != 256) { launch_reg_th<Real, N, CONTIG, MODE, Op, 256>(p, axis, op); return; } break;
+            case 512: if constexpr (512 % T == 0 && DEF != 512) { launch_reg_th<Real, N, CONTIG, MODE, Op, 512>(p, axis, op); return; } break;
+            default: break;
+        }
+    }
+    launch_reg_th<Real, N, CONTIG, MODE, Op, 0>(p, axis, op);
 }
 
 template <typename Real, bool CONTIG, int MODE, class Op>
@@ -196,6 +213,56 @@ static void kinetic_passes(gp5cu_plan *p, const void *src, void *w, const SolveP
     OpKinetic<Real> kin{(const V *)w, (V *)w, sp, p->shape[0], p->shape[1], p->shape[2]};
     launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
     launch_axis<Real, false, MODE_INV>(p, 1, cp);
+}
+
+template <typename Real> void Launch<Real>::autotune(gp5cu_plan *p, int nrep) {
+    using V = cpx<Real>;
+    V *w = (V *)p->work;
+    check_cuda(cudaMemsetAsync(w, 0, p->field_bytes * p->nsolve, p->stream), "memset work");
+    OpCopy<Real> cp{w, w, p->nsolve > 1 ? p->sp_lap : nullptr};
+    OpKinetic<Real> kin{w, w, p->sp_lap, p->shape[0], p->shape[1], p->shape[2]};
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    auto run = [&](int q) {
+        const int axis = kTunedAxis[q];
+        switch (kTunedMode[q]) {
+            case MODE_FWD: launch_axis<Real, false, MODE_FWD>(p, axis, cp); break;
+            case MODE_INV: launch_axis<Real, false, MODE_INV>(p, axis, cp); break;
+            default: launch_axis<Real, false, MODE_FWD_MID_INV>(p, axis, kin); break;
+        }
+    };
+    try {
+        for (int q = 0; q < kTunedPasses; q++) {
+            const int axis = kTunedAxis[q], mode = kTunedMode[q];
+            p->tile_threads[axis][mode] = 0;
+            if (!p->ax[axis].reg) continue;  // the shared-memory engine has one tile shape
+            float best = 0.f;
+            int best_th = 0;
+            for (int th : {128, 256, 512}) {
+                if (th % p->ax[axis].reg_threads != 0) continue;
+                p->tile_threads[axis][mode] = th;
+                run(q);  // configure and warm
+                check_cuda(cudaEventRecord(e0, p->stream), "cudaEventRecord");
+                for (int r = 0; r < nrep; r++) run(q);
+                check_cuda(cudaEventRecord(e1, p->stream), "cudaEventRecord");
+                check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+                float ms = 0.f;
+                check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                if (best_th == 0 || ms < best) {
+                    best = ms;
+                    best_th = th;
+                }
+            }
+            p->tile_threads[axis][mode] = best_th;
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 template <typename Real> void Launch<Real>::laplacian(gp5cu_plan *p, const void *src, void *dst) {

@@ -206,20 +206,25 @@ __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, 
 #ifndef GP5_HEAVY_THREADS
 #define GP5_HEAVY_THREADS 128
 #endif
-template <typename Real, int N, bool CONTIG, int MODE> struct RegTile {
+// TH > 0 overrides the rule (the autotuner's tile shapes for the strided y/z passes).
+template <typename Real, int N, bool CONTIG, int MODE, int TH = 0> struct RegTile {
     static constexpr int T = RegCfgAll<N>::T;
     static constexpr int THREADS =
-        (MODE == MODE_FWD_MID_INV || MODE == MODE_INV_TURN_FWD) && GP5_HEAVY_THREADS / T >= 2 ? GP5_HEAVY_THREADS : 256;
+        TH > 0 ? TH
+               : ((MODE == MODE_FWD_MID_INV || MODE == MODE_INV_TURN_FWD) && GP5_HEAVY_THREADS / T >= 2 ? GP5_HEAVY_THREADS
+                                                                                                      : 256);
+    static_assert(THREADS % T == 0 && THREADS <= 1024, "a tile is a whole number of lines");
     static constexpr int LINES = THREADS / T;
     // register cap: 128 per thread for complex128, 80 for complex64
-    static constexpr int MINB = (sizeof(Real) == 8 ? 65536 / 128 : 65536 / 80) / THREADS;
+    static constexpr int MINB_RAW = (sizeof(Real) == 8 ? 65536 / 128 : 65536 / 80) / THREADS;
+    static constexpr int MINB = MINB_RAW > 0 ? MINB_RAW : 1;
 };
 
-template <typename Real, int N, bool CONTIG, int MODE, class Op>
-__global__ void __launch_bounds__(RegTile<Real, N, CONTIG, MODE>::THREADS, RegTile<Real, N, CONTIG, MODE>::MINB)
+template <typename Real, int N, bool CONTIG, int MODE, class Op, int TH = 0>
+__global__ void __launch_bounds__(RegTile<Real, N, CONTIG, MODE, TH>::THREADS, RegTile<Real, N, CONTIG, MODE, TH>::MINB)
 k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedSlot rs) {
     using V = cpx<Real>;
-    constexpr int E = RegCfg<N>::E, T = RegCfgAll<N>::T, LINES = RegTile<Real, N, CONTIG, MODE>::LINES;
+    constexpr int E = RegCfg<N>::E, T = RegCfgAll<N>::T, LINES = RegTile<Real, N, CONTIG, MODE, TH>::LINES;
     constexpr int NB = Op::BATCH;
     static_assert(E % NB == 0, "batch must divide the elements per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];

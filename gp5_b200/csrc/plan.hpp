@@ -24,10 +24,17 @@ struct ProfRec {
 struct AxisPlan {
     int n = 0;
     bool reg = false;     // register engine (power of two in [32, 512])
+    int reg_threads = 0;  // register engine: threads per line
     LineSchedule sched{};  // mixed-radix schedule for the shared-memory engine
     void *tw = nullptr;    // device twiddle table, plan precision, forward sign
     int smem_lines = 0;    // lines per tile of the shared-memory engine
 };
+
+// The autotuned passes, in the order of gp5cu_plan_get_tiles: (axis, mode) of the strided
+// register-engine launches (y fwd, y inv, z fwd, z inv, z fwd*K^2*inv).
+constexpr int kTunedPasses = 5;
+constexpr int kTunedAxis[kTunedPasses] = {1, 1, 2, 2, 2};
+constexpr int kTunedMode[kTunedPasses] = {MODE_FWD, MODE_INV, MODE_FWD, MODE_INV, MODE_FWD_MID_INV};
 
 // Thrown inside the library, caught at the C boundary and turned into a status code.
 struct Gp5Error {
@@ -72,6 +79,9 @@ struct gp5cu_plan {
     int sms = 148;      // multiprocessors of the device
     gp5::ProfRec *prof = nullptr;
     bool dry = false;  // launch helpers only configure kernels (before a stream capture)
+    // threads per CTA of the register-engine passes along y/z, by [axis][mode] (0: the
+    // default rule); chosen by the autotuner when the plan is created
+    int tile_threads[3][4] = {};
 };
 
 struct gp5cu_functional {
@@ -119,6 +129,9 @@ template <typename Real> struct Launch {
     static int step_merged(gp5cu_stepper *st, void *field, bool prologue);
     static void prologue(gp5cu_stepper *st, void *field);  // forward x transform of psi
     static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
+    // times every tile shape of the strided y/z passes on the zeroed work field and keeps
+    // the fastest in p->tile_threads
+    static void autotune(gp5cu_plan *p, int nrep);
 };
 
 void set_scalars(cudaStream_t s, DevScalars *ds, int n = 1);
@@ -131,6 +144,7 @@ void build_axis_plan(gp5cu_plan *p, int d);
 void fill_functional_params(const gp5cu_plan *p, const gp5cu_functional_desc &d, gp5::SolveParams &S);
 void upload_params(const std::vector<gp5::SolveParams> &h, gp5::SolveParams **dptr);
 bool merged_path(const gp5cu_plan *p);
+void autotune_plan(gp5cu_plan *p, bool force);
 int queue_step(gp5cu_stepper *st, void *field, bool merged, bool prologue);
 void build_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps);
 void drop_graph(gp5cu_stepper *st);

@@ -246,6 +246,21 @@ int gp5cu_mlp_train(gp5cu_mlp *net, const float *x, const float *t, int count, i
 int gp5cu_gemm_bf16(const void *A, long long sam, long long sak, const void *B, long long sbn, long long sbk,
                     float *C, long long ldc, int M, int N, int K, void *stream);
 
+/* ---- tile-shape autotuner ----------------------------------------------------------------
+ * No reference counterpart (FFTW plans its own transforms).  The strided y/z passes of the
+ * register engine (axis lengths 32..512, powers of two) come in tile shapes of 128, 256 or 512
+ * threads per CTA (more threads = more consecutive x values per tile = wider coalesced rows).
+ * gp5cu_plan_create times every shape of the five passes below on the plan's zeroed work field
+ * and keeps the fastest; the choice is remembered per (device, shape, components, precision,
+ * solves) for the life of the process.  GP5_AUTOTUNE=0 in the environment keeps the default
+ * shapes.  These passes carry no reductions, so the tile shape changes no result bit.
+ * threads[5]: y forward, y inverse, z forward, z inverse, z forward*K^2*inverse; 0 = the
+ * default shape (or an axis that uses the shared-memory engine).  Steppers capture the shapes
+ * in their CUDA graphs when they first advance: set shapes before creating steppers. */
+int gp5cu_plan_autotune(gp5cu_plan *plan);
+int gp5cu_plan_get_tiles(const gp5cu_plan *plan, int threads[5]);
+int gp5cu_plan_set_tiles(gp5cu_plan *plan, const int threads[5]);
+
 /* ---- allocation-free norm ---------------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc when they need
  * a norm (their device memory belongs to another allocator, or the device is full): the same
