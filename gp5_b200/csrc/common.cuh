@@ -48,6 +48,17 @@ template <typename V> __host__ __device__ __forceinline__ V cconj(V a) {
     V r; r.x = a.x; r.y = -a.y; return r;
 }
 
+// ---- programmatic dependent launch ----------------------------------------------------
+// Every kernel of the stepper path starts here.  The wait returns once the grid this launch
+// depends on has completed and its writes are visible (at once when the launch has no
+// programmatic dependency), so nothing below reads a predecessor's output early; the trigger
+// then lets the next launch of the stream be scheduled while this grid drains.  The next
+// grid starts only after every CTA of this one has triggered, i.e. is resident or done.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---- status words shared with the host ------------------------------------------------
 enum DevStatus : unsigned { DS_OK = 0u, DS_NONFINITE = 1u, DS_TIMEOUT = 2u };
 

@@ -254,6 +254,10 @@ gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const do
         }
         p->ncomp = ncomp;
         p->prec = precision;
+        {
+            const char *pdl = std::getenv("GP5_PDL");
+            p->pdl = !(pdl && std::string(pdl) == "0");
+        }
         p->nsites = (long long)shape[0] * shape[1] * shape[2];
         p->nsolve = nsolve;
         p->solve_stride = p->nsites * ncomp;

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <utility>
 
 #include "ops.cuh"
 #include "plan.hpp"
@@ -60,6 +61,25 @@ void smem_opt_in(const void *kernel, size_t bytes, int dev);
 // CTAs of a kernel resident per SM (cached per kernel and device).
 int resident_blocks(const void *kernel, int threads, size_t smem, int dev);
 
+// Launch on the plan's stream with programmatic stream serialisation (unless the plan turned
+// it off): in a captured graph the launch gets a programmatic edge from its predecessor, and
+// the kernel's pdl_enter() keeps every read behind the predecessor's completion.
+template <typename... KArgs, typename... Args>
+inline void launch_k(const gp5cu_plan *p, void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem,
+                     Args &&...args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = p->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = p->pdl ? 1 : 0;
+    check_cuda(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...), "kernel launch");
+}
+
 template <class K> inline void ensure_smem(K kernel, size_t bytes, int dev) {
     if (bytes > 48 * 1024) smem_opt_in((const void *)kernel, bytes, dev);
 }
@@ -74,8 +94,7 @@ void launch_reg_th(gp5cu_plan *p, int axis, const Op &op) {
     auto kern = k_axis_reg<Real, N, CONTIG, MODE, Op, TH>;
     ensure_smem(kern, smem, p->dev);
     if (p->dry) return;
-    kern<<<(unsigned)tiles, THREADS, smem, p->stream>>>(g, op, (const V *)p->ax[axis].tw, red_slot(p));
-    check_cuda(cudaGetLastError(), "k_axis_reg launch");
+    launch_k(p, kern, (unsigned)tiles, THREADS, smem, g, op, (const V *)p->ax[axis].tw, red_slot(p));
     if (p->prof) p->prof->record(p->stream, axis * 10 + MODE);
 }
 
@@ -108,8 +127,7 @@ void launch_smem(gp5cu_plan *p, int axis, const Op &op) {
     auto kern = k_axis_smem<Real, CONTIG, MODE, Op>;
     ensure_smem(kern, smem, p->dev);
     if (p->dry) return;
-    kern<<<(unsigned)tiles, kThreads, smem, p->stream>>>(g, ap.sched, op, (const V *)ap.tw, red_slot(p));
-    check_cuda(cudaGetLastError(), "k_axis_smem launch");
+    launch_k(p, kern, (unsigned)tiles, kThreads, smem, g, ap.sched, op, (const V *)ap.tw, red_slot(p));
     if (p->prof) p->prof->record(p->stream, axis * 10 + MODE);
 }
 
@@ -143,8 +161,8 @@ void launch_axis(gp5cu_plan *p, int axis, const Op &op) {
 // Point-wise kernel over the sites of every solve: pw_bps blocks per solve.
 template <class Op> void launch_pointwise(gp5cu_plan *p, const Op &op) {
     if (p->dry) return;
-    k_pointwise<Op><<<p->pw_bps * p->nsolve, kThreads, 0, p->stream>>>(p->nsites, p->pw_bps, op, red_slot(p));
-    check_cuda(cudaGetLastError(), "k_pointwise launch");
+    launch_k(p, k_pointwise<Op>, (unsigned)(p->pw_bps * p->nsolve), kThreads, 0, p->nsites, p->pw_bps, op,
+             red_slot(p));
     if (p->prof) p->prof->record(p->stream, 90);
 }
 

@@ -230,6 +230,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *sm = reinterpret_cast<V *>(smem_raw);
 
+    pdl_enter();
     int tid, line;
     if (CONTIG) { tid = threadIdx.x % T; line = threadIdx.x / T; }
     else { line = threadIdx.x % LINES; tid = threadIdx.x / LINES; }
@@ -367,6 +368,7 @@ __global__ void __launch_bounds__(256)
 k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__restrict__ tw,
             const RedSlot rs) {
     using V = cpx<Real>;
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = g.n, lines = g.lines;
     const int ld = CONTIG ? n + 1 : lines;
@@ -454,6 +456,7 @@ k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__r
 // bps * blockDim.x.
 template <class Op>
 __global__ void __launch_bounds__(256) k_pointwise(const long long nsites, const int bps, Op op, const RedSlot rs) {
+    pdl_enter();
     constexpr int K = Op::NRED > 0 ? Op::NRED : 1;
     const int solve = blockIdx.x / bps;
     const int lb = blockIdx.x - solve * bps;

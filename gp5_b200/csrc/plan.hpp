@@ -82,6 +82,8 @@ struct gp5cu_plan {
     // threads per CTA of the register-engine passes along y/z, by [axis][mode] (0: the
     // default rule); chosen by the autotuner when the plan is created
     int tile_threads[3][4] = {};
+    // launches of the stepper path use programmatic dependent launch (GP5_PDL=0 turns it off)
+    bool pdl = true;
 };
 
 struct gp5cu_functional {
