@@ -150,6 +150,29 @@ template <typename Real> struct OpKinetic {
         const double k2 = __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
         return cscale(v, (Real)(k2 * S.kin[e.c]));
     }
+    // z lines: kx^2 + ky^2 is fixed along the line, so it is formed once and each element adds
+    // its own kz^2; kidx is kz's signed index.  complex128: the same operations in the same
+    // order as mid (bit-identical).  complex64: the per-element part runs in FP32 (one
+    // rounding of kx^2 + ky^2 per line; the factor's error stays below the transform's).
+    static constexpr bool MID_Z = true;
+    struct MidLine {
+        Real kxy2, dkz, kin;
+    };
+    __device__ __forceinline__ MidLine mid_line(const LineRef &e, const SolveCtx &X) const {
+        const SolveParams &S = X.S;
+        const double kx = momentum(S, 0, e.i, nx), ky = momentum(S, 1, e.j, ny);
+        return MidLine{(Real)__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), (Real)S.dk[2], (Real)S.kin[e.c]};
+    }
+    __device__ __forceinline__ V mid_z(V v, int kidx, const MidLine &L) const {
+        if constexpr (sizeof(Real) == 8) {
+            const double kz = __dmul_rn(L.dkz, (double)kidx);
+            const double k2 = __dadd_rn(L.kxy2, __dmul_rn(kz, kz));
+            return cscale(v, (Real)(k2 * L.kin));
+        } else {
+            const float kz = L.dkz * (float)kidx;
+            return cscale(v, (L.kxy2 + kz * kz) * L.kin);
+        }
+    }
     __device__ __forceinline__ Pre pre(long long) const { return Pre{}; }
     __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &, double *, const SolveCtx &) const {
         dst[g] = v;

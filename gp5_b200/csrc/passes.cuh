@@ -14,6 +14,8 @@
 // repeated runs are bitwise identical.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "fft_line.cuh"
 
@@ -197,6 +199,10 @@ __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, 
         prefetch_l2(reinterpret_cast<const V *>(st[q]) + e0, (unsigned)(cnt * sizeof(V)));
 }
 
+// ops that provide the hoisted z-line k-space multiply (mid_line / mid_z)
+template <class Op, class = void> struct has_mid_z : std::false_type {};
+template <class Op> struct has_mid_z<Op, std::void_t<decltype(Op::MID_Z)>> : std::true_type {};
+
 // ---- register-engine kernel ----------------------------------------------------------------
 // Threads: LINES lines x T threads per line (RegTile below); one tile per
 // CTA.
@@ -215,8 +221,13 @@ template <typename Real, int N, bool CONTIG, int MODE, int TH = 0> struct RegTil
                                                                                                       : 256);
     static_assert(THREADS % T == 0 && THREADS <= 1024, "a tile is a whole number of lines");
     static constexpr int LINES = THREADS / T;
-    // register cap: 128 per thread for complex128, 80 for complex64
-    static constexpr int MINB_RAW = (sizeof(Real) == 8 ? 65536 / 128 : 65536 / 80) / THREADS;
+    // register cap per thread: 128 for complex128.  complex64: the strided single-transform
+    // passes and the stage boundary are bound by memory latency and trade registers for
+    // resident CTAs (64: 8 CTAs of 128 threads, at most 8 bytes of spill); the other passes
+    // keep 80.  (A cap of 96 for the complex128 strided copies measured slower: it spills.)
+    static constexpr bool STRIDED_COPY = (MODE == MODE_FWD || MODE == MODE_INV) && !CONTIG;
+    static constexpr int REGCAP = sizeof(Real) == 8 ? 128 : (STRIDED_COPY || MODE == MODE_INV_TURN_FWD ? 64 : 80);
+    static constexpr int MINB_RAW = (65536 / REGCAP) / THREADS;
     static constexpr int MINB = MINB_RAW > 0 ? MINB_RAW : 1;
 };
 
@@ -317,7 +328,27 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
             LayStrided lay{LINES};
             if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
             else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
-            if (MODE == MODE_FWD_MID_INV) {
+            if constexpr (MODE == MODE_FWD_MID_INV && has_mid_z<Op>::value) {
+                if (g.axis == 2) {
+                    // element m sits at tid + T*m < N/2 exactly when m < E/2, so the sign of
+                    // its momentum index is known at compile time
+                    const auto L = op.mid_line(lr, X);
+#pragma unroll
+                    for (int m = 0; m < E; m++) {
+                        const int pos = tid + T * m;
+                        v[m] = op.mid_z(v[m], m < E / 2 ? pos : pos - N, L);
+                    }
+                } else {
+#pragma unroll
+                    for (int m = 0; m < E; m++) {
+                        LineRef e = lr;
+                        set_pos(g, e, tid + T * m);
+                        v[m] = op.mid(v[m], e, X);
+                    }
+                }
+                __syncthreads();  // also a scheduling fence: keeps register pressure below 128
+                reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+            } else if (MODE == MODE_FWD_MID_INV) {
 #pragma unroll
                 for (int m = 0; m < E; m++) {
                     LineRef e = lr;
