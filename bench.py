@@ -268,6 +268,74 @@ def roofline(r, dtype: str = "c128"):
             "per_kind_ms": {KIND_NAMES.get(k, str(k)): round(v[0], 4) for k, v in tot.items()}}
 
 
+# ---- precision report (complex64 bulk against complex128) ----------------------------------
+def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float = 1e-8):
+    """Ground state at c3 = -3 (imaginary-time RK4 to the residual tol, complex128), then the
+    quench c3 -> -3.3 in real time for `steps` RK4 steps of dt = 5e-5 in complex128 and in
+    complex64 from the same state; every `every` steps the norm and the energy of both (FP64
+    reductions) and the complex64 energy error against complex128."""
+    import numpy as np
+    import torch
+
+    from gp5_b200 import _abi
+
+    torch.cuda.set_device(dev)
+    shape, left, right = workload_geometry()
+    dx = (right[0] - left[0]) / N_GRID
+    p64 = _abi.Plan(shape, left, right, precision=_abi.GP5_C128, device=dev)
+    fgs = _abi.Functional(p64, _abi.GP5_FUNC_LHY, c3=-3.0, c4=C4)
+    sgs = _abi.Stepper(fgs, 0.15 * dx * dx, _abi.GP5_STEP_RK4, imaginary=True)
+    sgs.set_renormalization([N_ATOMS])
+    f = p64.field(initial_state())
+    t0 = time.perf_counter()
+    gs_steps = 0
+    ob = fgs.observables(f)
+    while ob["residual"] > tol and gs_steps < 100000:
+        sgs.advance(f, 500)
+        gs_steps += 500
+        ob = fgs.observables(f)
+    gs = {"steps": gs_steps, "residual": ob["residual"], "energy": ob["energy"], "mu": ob["mu"],
+          "seconds": round(time.perf_counter() - t0, 1)}
+    psi0 = f.download()
+    del f, sgs, fgs
+    rows = {}
+    f_eval = _abi.Functional(p64, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)  # complex128 evaluation
+    e_field = p64.field()
+    for prec, name in ((_abi.GP5_C128, "c128"), (_abi.GP5_C64, "c64")):
+        p = p64 if prec == _abi.GP5_C128 else _abi.Plan(shape, left, right, precision=prec, device=dev)
+        fq = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
+        sq = _abi.Stepper(fq, DT, _abi.GP5_STEP_RK4, imaginary=False)
+        g = p.field(psi0)
+        out = []
+        for k in range(0, steps + 1, every):
+            if k:
+                sq.advance(g, every)
+            o = fq.observables(g)
+            e128 = o["energy"]
+            if prec == _abi.GP5_C64:
+                # the complex64 state evaluated by the complex128 functional
+                e_field.upload(np.asarray(g.download(), dtype=np.complex128))
+                e128 = f_eval.observables(e_field)["energy"]
+            out.append((k, o["norm"], o["energy"], e128))
+        rows[name] = out
+        del g, sq, fq
+    table = []
+    n0, e0 = rows["c128"][0][1], rows["c128"][0][2]
+    for (k, n64, e64, _), (_, n32, e32, e32s) in zip(rows["c128"], rows["c64"]):
+        table.append({"step": k, "norm_c128": n64, "norm_c64": n32, "energy_c128": e64, "energy_c64": e32,
+                      "energy_c64_state_in_c128": e32s,
+                      "norm_drift_c128": (n64 - n0) / n0, "norm_drift_c64": (n32 - n0) / n0,
+                      "energy_rel_err_c64": abs(e32 - e64) / abs(e64),
+                      "energy_rel_err_c64_state": abs(e32s - e64) / abs(e64)})
+    return {"ground_state": gs, "checkpoints": table,
+            "max_energy_rel_err_c64": max(r["energy_rel_err_c64"] for r in table),
+            "max_energy_rel_err_c64_state": max(r["energy_rel_err_c64_state"] for r in table),
+            "max_norm_drift_c128": max(abs(r["norm_drift_c128"]) for r in table),
+            "max_norm_drift_c64": max(abs(r["norm_drift_c64"]) for r in table),
+            "workload": "N=5000 LHY droplet, 256^3, L=4 N^(1/3); ground state at c3=-3 (residual 1e-8), "
+                        "quench to c3=-3.3, real-time RK4 dt=5e-5"}
+
+
 # ---- batched droplet ground states (config: 64 seeded solves; bench leg: a seeded sample) ----
 def batch_solves(count: int, seed: int = 2025):
     """N log-uniform in [20, 2000], c3 ~ U[-3.2, -2.8], c4 = 2.5, no trap, L = 4 N^(1/3); grid:
@@ -359,6 +427,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision-report", metavar="JSON",
+                    help="also run the complex64-vs-complex128 quench report and write it here")
     ap.add_argument("--batch", type=int, default=16,
                     help="solves of the ground-state leg (0: skip; the full configuration is 64)")
     args = ap.parse_args()
@@ -398,6 +468,11 @@ def main():
                                              device_id=torch.device(f"cuda:{local_rank}"))
     results, launches = run_ours(args, rank, world, local_rank)
     gs = run_batch(args.batch, local_rank) if args.batch > 0 else None
+    prep = None
+    if args.precision_report and world == 1:
+        prep = precision_report(local_rank)
+        with open(args.precision_report, "w") as fh:
+            json.dump(prep, fh, indent=1)
     if world > 1:
         import torch
 
@@ -416,7 +491,11 @@ def main():
             "data": "synthetic", "config": config,
             "fp32": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "dtype": "c64",
                      "speedup_vs_fp64": r32["value"] / r64["value"], "clocks": r32["clocks"],
-                     "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2), "c64")},
+                     "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2), "c64"),
+                     "energy_error": ({k: prep[k] for k in ("max_energy_rel_err_c64", "max_energy_rel_err_c64_state",
+                                                            "max_norm_drift_c64",
+                                                            "max_norm_drift_c128")} if prep else
+                                      "profiles/precision_quench_256cubed.md")},
             "e2e": r64["e2e"], "roofline": roofline(r64, "c128"), "cpu_baseline": cpu,
             "clocks": r64["clocks"], "gpu_launches": launches,
             "autotune": {"passes": ["y_fwd", "y_inv", "z_fwd", "z_inv", "z_fwd_kinetic_inv"],

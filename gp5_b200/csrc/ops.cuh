@@ -345,9 +345,8 @@ __device__ __forceinline__ void apply_functional(const EpiParams<Real> &P, const
     }
 }
 
-template <typename Real, int NC>
-__device__ __forceinline__ double interaction_energy(const EpiParams<Real> &P, const SolveParams &S,
-                                                     const Real (&nn)[NC]) {
+template <typename D, int NC, class EP>
+__device__ __forceinline__ double interaction_energy(const EP &P, const SolveParams &S, const D (&nn)[NC]) {
     if (P.fkind == FK_GP) {
         if (!P.has_g) return 0.0;
         if (NC == 1) return 0.5 * S.g00 * (double)nn[0] * (double)nn[0];
@@ -425,7 +424,15 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
                 acc[2] += (double)Vv[c] * (ur * ur + ui * ui);
                 acc[4] += ur * (double)h[c].x + ui * (double)h[c].y;
             }
-            acc[3] += interaction_energy<Real, NC>(P, S, nn);
+            if constexpr (sizeof(Real) == 8) {
+                acc[3] += interaction_energy<Real, NC>(P, S, nn);
+            } else {
+                // complex64: the densities of the energy sum are formed in FP64
+                double nd[NC];
+#pragma unroll
+                for (int c = 0; c < NC; c++) nd[c] = (double)u[c].x * u[c].x + (double)u[c].y * u[c].y;
+                acc[3] += interaction_energy<double, NC>(P, S, nd);
+            }
         }
         return;
     }
