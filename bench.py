@@ -156,6 +156,28 @@ def ncu_traffic(kind_name: str, dtype: str):
     return None
 
 
+def _reduce(x: float, world: int, op: str) -> float:
+    """x reduced over the ranks of the default process group (MAX or SUM); a CPU tensor under
+    gloo, a CUDA tensor under NCCL.  Every rank must call it, in the same order."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    return _reduce(x, world, "max")
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    return _reduce(x, world, "sum")
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -188,11 +210,7 @@ def run_ours(args, rank, world, local_rank):
                 st.advance(f, args.steps)
                 e1.record(stream)
                 torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1)
-            if world > 1:
-                t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
-                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-                ms = float(t.item())
+            ms = max_over_ranks(e0.elapsed_time(e1), world)
         lps = st.launches_per_step
         launches += lps * args.steps + 1  # + the prologue transform of each advance call
         r = {"ms": ms, "ms_per_step": ms / args.steps, "value": world * sites * args.steps / (ms / 1e3),
@@ -216,11 +234,7 @@ def run_ours(args, rank, world, local_rank):
                     st.advance_host(host_in.numpy(), host_out.numpy(), 1)
                 e1.record(stream)
                 torch.cuda.synchronize()
-                ems = e0.elapsed_time(e1)
-                if world > 1:
-                    t = torch.tensor([ems], device=f"cuda:{dev}", dtype=torch.float64)
-                    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-                    ems = float(t.item())
+                ems = max_over_ranks(e0.elapsed_time(e1), world)
             launches += (lps + 1) * n_e2e
             r["e2e"] = {"value": world * sites * n_e2e / (ems / 1e3), "unit": "site-updates/s",
                         "h2d_bytes_per_step": plan.field_bytes, "d2h_bytes_per_step": plan.field_bytes,
@@ -337,14 +351,15 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
 
 
 # ---- batched droplet ground states (config: 64 seeded solves; bench leg: a seeded sample) ----
-def batch_solves(count: int, seed: int = 2025):
+def batch_solves(count: int, seed: int = 2025, rank: int = 0):
     """N log-uniform in [20, 2000], c3 ~ U[-3.2, -2.8], c4 = 2.5, no trap, L = 4 N^(1/3); grid:
     the smallest of 32^3/64^3/128^3 with L/n <= 0.25, else 128^3 (N > 512 cannot meet the
     spacing on these grids); dt = 0.15 dx^2 (RK4 is stable on the cube-corner modes
     K^2 = 3 (pi/dx)^2 up to dt = 0.188 dx^2)."""
     import numpy as np
 
-    rng = np.random.default_rng(seed)
+    # each rank draws its own shard of droplets (independent solves: no data-path collective)
+    rng = np.random.default_rng([seed, rank])
     out = []
     for _ in range(count):
         N = float(np.exp(rng.uniform(math.log(20.0), math.log(2000.0))))
@@ -369,32 +384,36 @@ def droplet_state(sd, seed):
     return np.asfortranarray(psi)
 
 
-def run_batch(count: int, dev: int, tol: float = 1e-8):
+def run_batch(count: int, dev: int, tol: float = 1e-8, rank: int = 0, world: int = 1):
     import torch
 
     from gp5_b200 import _abi
 
-    solves = batch_solves(count)
+    solves = batch_solves(count, rank=rank)
     b = _abi.Batch(solves, precision=_abi.GP5_C128, device=dev)
     for k, sd in enumerate(solves):
-        b.set_state(k, droplet_state(sd, 3000 + k))
+        b.set_state(k, droplet_state(sd, 3000 + 1000 * rank + k))
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     t0 = time.perf_counter()
     res = b.solve(tol=tol, check_every=500, max_steps=400000)
-    wall = time.perf_counter() - t0
-    conv = sum(r["converged"] for r in res)
-    site_steps = sum(r["steps"] * sd["n"] ** 3 for r, sd in zip(res, solves))
+    wall = max_over_ranks(time.perf_counter() - t0, world)
+    conv = int(sum_over_ranks(sum(r["converged"] for r in res), world))
+    site_steps = sum_over_ranks(sum(r["steps"] * sd["n"] ** 3 for r, sd in zip(res, solves)), world)
+    launches = int(sum_over_ranks(b.launches, world))
     grids = {}
     for sd in solves:
         grids[str(sd["n"])] = grids.get(str(sd["n"]), 0) + 1
-    return {"value": conv / wall, "unit": "ground states/s", "solves": count, "converged": conv, "tol": tol,
-            "seconds": wall, "dtype": "c128", "grids": grids,
-            "steps": {"min": min(r["steps"] for r in res), "max": max(r["steps"] for r in res),
-                      "mean": sum(r["steps"] for r in res) / count},
-            "site_updates_per_s": site_steps / wall, "gpu_launches": b.launches,
-            "workload": "seeded LHY droplets: N log-uniform [20,2000], c3 U[-3.2,-2.8], c4 2.5, "
-                        "Gaussian start (width 0.5 N^(1/3), phase noise 1e-3), imaginary-time RK4 "
-                        "renormalised every step, dt 0.15 dx^2, residual checked every 500 steps"}
+    return {"value": conv / wall, "unit": "ground states/s", "solves": count * world, "converged": conv,
+            "tol": tol, "seconds": wall, "dtype": "c128", "grids_rank0": grids,
+            "steps_rank0": {"min": min(r["steps"] for r in res), "max": max(r["steps"] for r in res),
+                            "mean": sum(r["steps"] for r in res) / count},
+            "site_updates_per_s": site_steps / wall, "gpu_launches": launches,
+            "workload": "seeded LHY droplets (one shard of " + str(count) + " per rank): N log-uniform "
+                        "[20,2000], c3 U[-3.2,-2.8], c4 2.5, Gaussian start (width 0.5 N^(1/3), phase "
+                        "noise 1e-3), imaginary-time RK4 renormalised every step, dt 0.15 dx^2, residual "
+                        "checked every 500 steps"}
 
 
 def cpu_reference_timing(max_seconds: float, max_steps: int, warm: bool = True):
@@ -467,7 +486,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
     results, launches = run_ours(args, rank, world, local_rank)
-    gs = run_batch(args.batch, local_rank) if args.batch > 0 else None
+    gs = run_batch(args.batch, local_rank, rank=rank, world=world) if args.batch > 0 else None
     prep = None
     if args.precision_report and world == 1:
         prep = precision_report(local_rank)
