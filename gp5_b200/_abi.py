@@ -131,6 +131,8 @@ def lib():
         "gp5cu_batch_get_state": (i, [vp, i, vp]),
         "gp5cu_batch_solve": (i, [vp, d, i, i, C.POINTER(SolveResult)]),
         "gp5cu_batch_launches": (C.c_longlong, [vp]),
+        "gp5cu_decompose": (i, [vp, vp, i, d, vp, C.POINTER(C.c_int)]),
+        "gp5cu_decompose_host": (i, [vp, vp, i, d, vp, C.POINTER(C.c_int)]),
         "gp5cu_plan_autotune": (i, [vp]),
         "gp5cu_plan_get_tiles": (i, [vp, C.POINTER(C.c_int)]),
         "gp5cu_plan_set_tiles": (i, [vp, C.POINTER(C.c_int)]),
@@ -215,6 +217,15 @@ class Plan:
         out = C.c_double()
         check(lib().gp5cu_max_density(self.h, f.ptr, C.byref(out)))
         return out.value
+
+    def decompose(self, f: "DeviceField", cutoff: float, comp: int = 0):
+        """Droplet labels (gp5cu_decompose_host): int32 (nx, ny, nz, ncomp), Fortran order, and
+        the number of clusters."""
+        out = np.empty(self.field_shape, dtype=np.int32, order="F")
+        k = C.c_int()
+        check(lib().gp5cu_decompose_host(self.h, f.ptr, int(comp), float(cutoff), C.c_void_p(_ptr(out)),
+                                         C.byref(k)))
+        return out, k.value
 
     def tiles(self):
         """Threads per CTA of (y fwd, y inv, z fwd, z inv, z fwd*K^2*inv); 0 = default shape."""

@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                   "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["gp5cu_f64.cu", "gp5cu_f32.cu", "gp5cu_host.cu", "gp5cu_batch.cu", "gp5cu_noalloc.cu", "mlp.cu"]
+CU_SOURCES = ["gp5cu_f64.cu", "gp5cu_f32.cu", "gp5cu_host.cu", "gp5cu_batch.cu", "gp5cu_noalloc.cu", "mlp.cu", "gp5cu_cluster.cu"]
 HEADERS = ["common.cuh", "fft_line.cuh", "passes.cuh", "ops.cuh", "launch_impl.cuh", "plan.hpp"]
 
 

@@ -134,6 +134,20 @@ private:
     void *_d = nullptr;
 };
 
+// gpCpp.cpp:289-313: labels of the droplets of component 0 with density above the cutoff
+class decomposition {
+public:
+    py::array_t<int> decompose(const field &psi, double densityCutOff) {
+        const auto s = psi.geo().getShape();
+        const py::ssize_t nx = s[0], ny = s[1], nz = s[2], nc = psi.nComponents();
+        const py::ssize_t e = sizeof(int);
+        py::array_t<int> a({nx, ny, nz, nc}, {e, e * nx, e * nx * ny, e * nx * ny * nz});
+        int k = 0;
+        check(gp5cu_decompose_host(psi.plan(), psi.data(), 0, densityCutOff, a.mutable_data(), &k));
+        return a;
+    }
+};
+
 class model {
 public:
     virtual ~model() {
@@ -304,6 +318,9 @@ PYBIND11_MODULE(gpCpp, m) {
         .def(py::init<field &, std::vector<std::vector<double>>, std::vector<double>, std::vector<arr3d>>(),
              py::arg("psi"), py::arg("couplings") = std::vector<std::vector<double>>{},
              py::arg("masses") = std::vector<double>{}, py::arg("omegas") = std::vector<arr3d>{});
+    py::class_<decomposition>(m, "decomposition")
+        .def(py::init<>())
+        .def("decompose", &decomposition::decompose, py::arg("psi"), py::arg("densityCutOff"));
     py::class_<timeStepper>(m, "timeStepper")
         .def(py::init<double, std::string, bool>())
         .def("setRenormalization", &timeStepper::setRenormalization)

@@ -216,6 +216,18 @@ int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps
 /* Kernel launches of the last gp5cu_batch_solve call. */
 long long gp5cu_batch_launches(const gp5cu_batch *b);
 
+/* ---- droplet decomposition --------------------------------------------------------------
+ * gp::decompose::decompose (src/cluster.cpp:17-83) behind the gpCpp `decomposition` class
+ * (src/gpCpp.cpp:289-313): labels (int32, the field's layout (nx, ny, nz, ncomp)) of the
+ * connected components of the sites of component `comp` with |psi|^2 > cutoff, 26-connected,
+ * periodic; sites at or below the cutoff get -1, the other components 0; clusters are numbered
+ * from 1 in the order in which a scan over (i, j, k), i slowest, meets their first site.
+ * *nclusters receives their number.  Plans of one solve only.  dlabels: device memory;
+ * gp5cu_decompose_host writes host memory (and allocates a device label buffer for the call). */
+int gp5cu_decompose(gp5cu_plan *plan, const void *dfield, int comp, double cutoff, int *dlabels, int *nclusters);
+int gp5cu_decompose_host(gp5cu_plan *plan, const void *dfield, int comp, double cutoff, int *labels,
+                         int *nclusters);
+
 /* ---- learned warm start ------------------------------------------------------------------
  * No counterpart in the reference, which starts every solve from a Gaussian
  * (python/test/regressionTests/LHY_imaginary.py:14).  A 3 -> 256 -> 256 -> 256 -> 64 MLP with

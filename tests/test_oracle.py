@@ -143,3 +143,32 @@ def test_rk4_imaginary_stability_bound_on_corner_modes():
         e1 = o.observables(f, st.advance(psi.copy(), 300), geo)["ekin"]
         grow.append(e1 / e0)
     assert grow[0] < 1.0 and grow[1] > 3.0
+
+
+def test_decompose_squares_reference_case():
+    # tst/cluster_test.cpp:34-58 on the oracle's restatement of src/cluster.cpp:17-83
+    import oracle
+    data = np.zeros((100, 100, 100, 1), complex)
+    data[10:51, 10:51, 10:51, 0] = 1
+    lab, k = oracle.decompose(data, 0.5)
+    assert k == 1 and (lab[10:51, 10:51, 10:51] == 1).all()
+    assert (lab[0:10] == -1).all() and (lab[51:] == -1).all()
+    data[:] = 0
+    data[10:21, 10:21, 10:21] = 1
+    data[50:61, 10:21, 10:21] = 1
+    lab, k = oracle.decompose(data, 0.5)
+    assert k == 2 and (lab[10:21, 10:21, 10:21] == 1).all() and (lab[50:61, 10:21, 10:21] == 2).all()
+
+
+def test_decompose_periodic_diagonal_order_and_cutoff():
+    import oracle
+    d = np.zeros((12, 10, 8, 2), complex)
+    d[0, 3, 3, 0] = d[11, 3, 3, 0] = 1           # joined through the x boundary
+    d[5, 5, 5, 0] = d[6, 6, 6, 0] = 1            # joined through a corner (26-neighbours)
+    d[2, 0, 0, 0] = 1                            # scanned before (5,...) with i slowest
+    d[8, 9, 7, 0] = 0.5 + 0.5j                   # |psi|^2 = 0.5: not above the cutoff
+    lab, k = oracle.decompose(d, 0.5)
+    assert k == 3
+    assert lab[0, 3, 3, 0] == lab[11, 3, 3, 0] == 1
+    assert lab[2, 0, 0, 0] == 2 and lab[5, 5, 5, 0] == lab[6, 6, 6, 0] == 3
+    assert lab[8, 9, 7, 0] == -1 and (lab[..., 1] == 0).all()
