@@ -4,6 +4,9 @@
 // entry point catches the library's internal errors and returns a status code; the message
 // is kept per thread for gp5cu_last_error().
 #include <array>
+#include <cstdio>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -209,27 +212,119 @@ static SolveParams geometry_params(const int shape[3], const double left[3], con
 }
 
 // A plan for nsolve independent solves of one grid (boxes may differ per solve).
-// Tile shapes chosen by the autotuner, per (device, shape, components, precision, solves).
-// GP5_AUTOTUNE=0 in the environment keeps the default shapes.
+// Tile shapes chosen by the autotuner, per (device model, shape, components, precision,
+// solves), kept in memory and in a JSON file: GP5_AUTOTUNE_CACHE names it (empty: no file),
+// default $XDG_CACHE_HOME/gp5_b200/autotune.json or ~/.cache/gp5_b200/autotune.json.  The file
+// maps "<device>|<nx>x<ny>x<nz>|c<ncomp>|<c128|c64>|s<nsolve>|build <date time>" to the five thread counts of
+// gp5cu_plan_get_tiles.  GP5_AUTOTUNE=0 keeps the default shapes.
 static std::mutex g_tune_mu;
-static std::map<std::array<long long, 7>, std::array<int, 12>> g_tune_cache;
+static std::map<std::string, std::array<int, kTunedPasses>> g_tune_cache;
+static bool g_tune_loaded = false;
+
+static std::string tune_cache_path() {
+    const char *e = std::getenv("GP5_AUTOTUNE_CACHE");
+    if (e) return std::string(e);
+    const char *x = std::getenv("XDG_CACHE_HOME");
+    if (x && *x) return std::string(x) + "/gp5_b200/autotune.json";
+    const char *h = std::getenv("HOME");
+    if (h && *h) return std::string(h) + "/.cache/gp5_b200/autotune.json";
+    return std::string();
+}
+
+// reads entries "key": [a, b, c, d, e]; anything else in the file is skipped
+static void tune_cache_load(const std::string &path) {
+    FILE *f = path.empty() ? nullptr : std::fopen(path.c_str(), "rb");
+    if (!f) return;
+    std::string txt;
+    char buf[4096];
+    size_t n;
+    while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) txt.append(buf, n);
+    std::fclose(f);
+    size_t pos = 0;
+    while ((pos = txt.find('"', pos)) != std::string::npos) {
+        const size_t end = txt.find('"', pos + 1);
+        if (end == std::string::npos) break;
+        const std::string key = txt.substr(pos + 1, end - pos - 1);
+        size_t q = txt.find_first_not_of(" \t\r\n:", end + 1);
+        if (q == std::string::npos || txt[q] != '[') {
+            pos = end + 1;
+            continue;
+        }
+        std::array<int, kTunedPasses> v{};
+        bool ok = true;
+        const char *c = txt.c_str() + q + 1;
+        for (int t = 0; t < kTunedPasses && ok; t++) {
+            char *next = nullptr;
+            const long x = std::strtol(c, &next, 10);
+            if (next == c || !(x == 0 || x == 128 || x == 256 || x == 512)) ok = false;
+            v[t] = (int)x;
+            c = next;
+            while (*c == ' ' || *c == ',' || *c == '\n' || *c == '\t' || *c == '\r') c++;
+        }
+        if (ok) g_tune_cache[key] = v;
+        pos = end + 1;
+    }
+}
+
+static void tune_cache_store(const std::string &path) {
+    if (path.empty()) return;
+    const size_t slash = path.find_last_of('/');
+    if (slash != std::string::npos) {  // create the directory chain
+        for (size_t p = 1; p <= slash; p++)
+            if (path[p] == '/' || p == slash) mkdir(path.substr(0, p == slash ? slash : p).c_str(), 0755);
+    }
+    const std::string tmp = path + ".tmp." + std::to_string((long)getpid());
+    FILE *f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return;  // the cache is an optimisation: a read-only location just keeps it in memory
+    std::fprintf(f, "{\n");
+    size_t i = 0;
+    for (const auto &kv : g_tune_cache) {
+        std::fprintf(f, "  \"%s\": [%d, %d, %d, %d, %d]%s\n", kv.first.c_str(), kv.second[0], kv.second[1],
+                     kv.second[2], kv.second[3], kv.second[4], ++i < g_tune_cache.size() ? "," : "");
+    }
+    std::fprintf(f, "}\n");
+    std::fclose(f);
+    std::rename(tmp.c_str(), path.c_str());
+}
+
+static std::string tune_key(const gp5cu_plan *p) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, p->dev);
+    std::string name(prop.name);
+    for (char &ch : name)
+        if (ch == '"' || ch == '|' || ch == '\\') ch = '_';
+    return name + "|" + std::to_string(p->shape[0]) + "x" + std::to_string(p->shape[1]) + "x" +
+           std::to_string(p->shape[2]) + "|c" + std::to_string(p->ncomp) + "|" +
+           (p->prec == GP5_C128 ? "c128" : "c64") + "|s" + std::to_string(p->nsolve) +
+           "|build " __DATE__ " " __TIME__;  // another build tunes afresh
+}
 
 void autotune_plan(gp5cu_plan *p, bool force) {
     const char *env = std::getenv("GP5_AUTOTUNE");
     if (!force && env && std::string(env) == "0") return;
-    const std::array<long long, 7> key{p->dev, p->shape[0], p->shape[1], p->shape[2], p->ncomp, p->prec, p->nsolve};
     std::lock_guard<std::mutex> lk(g_tune_mu);
+    const std::string path = tune_cache_path();
+    if (!g_tune_loaded) {
+        tune_cache_load(path);
+        g_tune_loaded = true;
+    }
+    const std::string key = tune_key(p);
     auto it = g_tune_cache.find(key);
     if (!force && it != g_tune_cache.end()) {
-        std::memcpy(p->tile_threads, it->second.data(), sizeof(p->tile_threads));
+        for (int q = 0; q < kTunedPasses; q++) {
+            const int t = it->second[q];
+            const AxisPlan &ap = p->ax[kTunedAxis[q]];
+            p->tile_threads[kTunedAxis[q]][kTunedMode[q]] = (t != 0 && ap.reg && t % ap.reg_threads == 0) ? t : 0;
+        }
         return;
     }
     if (p->prec == GP5_C128) Launch<double>::autotune(p, 3);
     else Launch<float>::autotune(p, 3);
     check_cuda(cudaStreamSynchronize(p->stream), "sync");
-    std::array<int, 12> v{};
-    std::memcpy(v.data(), p->tile_threads, sizeof(p->tile_threads));
+    std::array<int, kTunedPasses> v{};
+    for (int q = 0; q < kTunedPasses; q++) v[q] = p->tile_threads[kTunedAxis[q]][kTunedMode[q]];
     g_tune_cache[key] = v;
+    tune_cache_store(path);
 }
 
 gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const double *const *rights, int nsolve,

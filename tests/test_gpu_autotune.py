@@ -67,3 +67,26 @@ def test_set_tiles_rejects_bad_shapes():
         p.set_tiles([256, 0, 0, 0, 0])  # y = 50 uses the shared-memory engine
     p.set_tiles([0, 0, 256, 256, 256])
     assert p.tiles() == [0, 0, 256, 256, 256]
+
+
+def test_tuning_cache_file_is_written_and_reused(tmp_path):
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    path = tmp_path / "tune.json"
+    code = ("import sys; sys.path.insert(0, %r); from gp5_b200 import _abi; "
+            "p = _abi.Plan((64, 64, 64), (-1.0,) * 3, (1.0,) * 3); print(p.tiles())" % root)
+    env = dict(os.environ, GP5_AUTOTUNE_CACHE=str(path))
+    r1 = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r1.returncode == 0, r1.stderr
+    d = json.loads(path.read_text())
+    keys = [k for k in d if "|64x64x64|c1|c128|s1|" in k]
+    assert len(keys) == 1 and d[keys[0]] == eval(r1.stdout.strip().splitlines()[-1])
+    d[keys[0]] = [512, 256, 512, 256, 256]
+    path.write_text(json.dumps(d))
+    r2 = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert r2.returncode == 0, r2.stderr
+    assert eval(r2.stdout.strip().splitlines()[-1]) == [512, 256, 512, 256, 256]
