@@ -192,11 +192,13 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream(device=dev)
     results = {}
     launches = 0
-    for prec in (_abi.GP5_C128, _abi.GP5_C64):
+    for key, prec, comp in ((0, _abi.GP5_C128, False), (1, _abi.GP5_C64, False), (2, _abi.GP5_C64, True)):
         plan = _abi.Plan(shape, left, right, precision=prec, device=dev)
         plan.set_stream(stream.cuda_stream)
         func = _abi.Functional(plan, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
         st = _abi.Stepper(func, DT, _abi.GP5_STEP_RK4, imaginary=False)
+        if comp:
+            st.set_compensation(True)
         f = plan.field(psi0)
         st.advance(f, args.warmup)  # builds the step graph; W untimed steps
         with torch.cuda.stream(stream):
@@ -240,7 +242,7 @@ def run_ours(args, rank, world, local_rank):
                         "h2d_bytes_per_step": plan.field_bytes, "d2h_bytes_per_step": plan.field_bytes,
                         "steps": n_e2e, "ms_per_step": ems / n_e2e}
             r["field_bytes"] = plan.field_bytes
-        results[prec] = r
+        results[key] = r
         del f, st, func, plan
         torch.cuda.synchronize()
     return results, launches
@@ -315,15 +317,31 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
     rows = {}
     f_eval = _abi.Functional(p64, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)  # complex128 evaluation
     e_field = p64.field()
-    for prec, name in ((_abi.GP5_C128, "c128"), (_abi.GP5_C64, "c64")):
-        p = p64 if prec == _abi.GP5_C128 else _abi.Plan(shape, left, right, precision=prec, device=dev)
+    p32 = None
+    ms_adv = {}
+    for prec, name, comp in ((_abi.GP5_C128, "c128", False), (_abi.GP5_C64, "c64", False),
+                             (_abi.GP5_C64, "c64c", True)):
+        if prec == _abi.GP5_C128:
+            p = p64
+        else:
+            p32 = p32 or _abi.Plan(shape, left, right, precision=prec, device=dev)
+            p = p32
         fq = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
         sq = _abi.Stepper(fq, DT, _abi.GP5_STEP_RK4, imaginary=False)
+        if comp:
+            sq.set_compensation(True)
         g = p.field(psi0)
         out = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tms = []
         for k in range(0, steps + 1, every):
             if k:
+                torch.cuda.synchronize()
+                e0.record()
                 sq.advance(g, every)
+                e1.record()
+                torch.cuda.synchronize()
+                tms.append(e0.elapsed_time(e1) / every)
             o = fq.observables(g)
             e128 = o["energy"]
             if prec == _abi.GP5_C64:
@@ -332,16 +350,21 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
                 e128 = f_eval.observables(e_field)["energy"]
             out.append((k, o["norm"], o["energy"], e128))
         rows[name] = out
+        ms_adv[name] = sorted(tms)[len(tms) // 2] if tms else None  # median ms per step (graph, warm)
         del g, sq, fq
     table = []
-    n0, e0 = rows["c128"][0][1], rows["c128"][0][2]
-    for (k, n64, e64, _), (_, n32, e32, e32s) in zip(rows["c128"], rows["c64"]):
-        table.append({"step": k, "norm_c128": n64, "norm_c64": n32, "energy_c128": e64, "energy_c64": e32,
-                      "energy_c64_state_in_c128": e32s,
+    n0 = rows["c128"][0][1]
+    for (k, n64, e64, _), (_, n32, e32, e32s), (_, nc, ec, ecs) in zip(rows["c128"], rows["c64"], rows["c64c"]):
+        table.append({"step": k, "norm_c128": n64, "norm_c64": n32, "norm_c64c": nc, "energy_c128": e64,
+                      "energy_c64": e32, "energy_c64c": ec, "energy_c64_state_in_c128": e32s,
                       "norm_drift_c128": (n64 - n0) / n0, "norm_drift_c64": (n32 - n0) / n0,
+                      "norm_drift_c64c": (nc - n0) / n0,
                       "energy_rel_err_c64": abs(e32 - e64) / abs(e64),
-                      "energy_rel_err_c64_state": abs(e32s - e64) / abs(e64)})
-    return {"ground_state": gs, "checkpoints": table,
+                      "energy_rel_err_c64_state": abs(e32s - e64) / abs(e64),
+                      "energy_rel_err_c64c": abs(ec - e64) / abs(e64)})
+    return {"ground_state": gs, "checkpoints": table, "ms_per_step_median": ms_adv,
+            "max_energy_rel_err_c64c": max(r["energy_rel_err_c64c"] for r in table),
+            "max_norm_drift_c64c": max(abs(r["norm_drift_c64c"]) for r in table),
             "max_energy_rel_err_c64": max(r["energy_rel_err_c64"] for r in table),
             "max_energy_rel_err_c64_state": max(r["energy_rel_err_c64_state"] for r in table),
             "max_norm_drift_c128": max(abs(r["norm_drift_c128"]) for r in table),
@@ -499,7 +522,7 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
-    r64, r32 = results[0], results[1]
+    r64, r32, r32c = results[0], results[1], results[2]
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         c = cpu_reference_timing(max_seconds=20.0, max_steps=4, warm=False)
@@ -512,9 +535,14 @@ def main():
                      "speedup_vs_fp64": r32["value"] / r64["value"], "clocks": r32["clocks"],
                      "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2), "c64"),
                      "energy_error": ({k: prep[k] for k in ("max_energy_rel_err_c64", "max_energy_rel_err_c64_state",
-                                                            "max_norm_drift_c64",
+                                                            "max_energy_rel_err_c64c", "max_norm_drift_c64c",
+                                                            "ms_per_step_median", "max_norm_drift_c64",
                                                             "max_norm_drift_c128")} if prep else
-                                      "profiles/precision_quench_256cubed.md")},
+                                      "profiles/precision_quench_256cubed.md"),
+                     "compensated": {"value": r32c["value"], "ms_per_step": r32c["ms_per_step"],
+                                     "speedup_vs_fp64": r32c["value"] / r64["value"], "clocks": r32c["clocks"],
+                                     "note": "gp5cu_stepper_set_compensation: BF16 correction field, "
+                                             "two-sum state update"}},
             "e2e": r64["e2e"], "roofline": roofline(r64, "c128"), "cpu_baseline": cpu,
             "clocks": r64["clocks"], "gpu_launches": launches,
             "autotune": {"passes": ["y_fwd", "y_inv", "z_fwd", "z_inv", "z_fwd_kinetic_inv"],

@@ -118,6 +118,7 @@ def lib():
         "gp5cu_stepper_destroy": (i, [vp]),
         "gp5cu_stepper_set_renormalization": (i, [vp, i, C.POINTER(d)]),
         "gp5cu_stepper_set_phase_constraint": (i, [vp, vp]),
+        "gp5cu_stepper_set_compensation": (i, [vp, i]),
         "gp5cu_stepper_advance": (i, [vp, vp, i]),
         "gp5cu_stepper_get_time": (i, [vp, C.POINTER(d)]),
         "gp5cu_stepper_set_time": (i, [vp, d]),
@@ -379,6 +380,10 @@ class Stepper:
         else:
             arr = (C.c_double * len(N))(*N)
             check(lib().gp5cu_stepper_set_renormalization(self.h, len(N), arr))
+
+    def set_compensation(self, on: bool) -> None:
+        """Compensated complex64 state update (gp5cu_stepper_set_compensation)."""
+        check(lib().gp5cu_stepper_set_compensation(self.h, 1 if on else 0))
 
     def set_phase_constraint(self, phase: Optional[DeviceField]) -> None:
         check(lib().gp5cu_stepper_set_phase_constraint(self.h, phase.ptr if phase is not None else None))

@@ -795,6 +795,7 @@ int gp5cu_stepper_destroy(gp5cu_stepper *st) {
     cudaFree(st->ds);
     cudaFree(st->phase_exp);
     cudaFree(st->dstate);
+    cudaFree(st->comp);
     cudaFree(st->sp);
     delete st;
     return GP5_OK;
@@ -828,6 +829,28 @@ int gp5cu_stepper_set_renormalization(gp5cu_stepper *st, int n, const double *N)
     }
     upload_params(st->sp_host, &st->sp);
     drop_graph(st);
+    GP5_CATCH
+}
+
+int gp5cu_stepper_set_compensation(gp5cu_stepper *st, int on) {
+    GP5_TRY
+    require(st != nullptr, "stepper is NULL");
+    gp5cu_plan *p = st->func->plan;
+    if (on) require(p->prec == GP5_C64, "the compensated update is for complex64 plans");
+    use_device(p);
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    drop_graph(st);
+    if (on) {
+        const size_t bytes = p->field_bytes / 2 * (size_t)p->nsolve;  // BF16 pair per element
+        if (!st->comp) check_cuda(cudaMalloc(&st->comp, bytes), "cudaMalloc compensation");
+        check_cuda(cudaMemset(st->comp, 0, bytes), "memset compensation");
+        st->compensate = true;
+    } else {
+        cudaFree(st->comp);
+        st->comp = nullptr;
+        st->compensate = false;
+    }
+    st->comp_field = nullptr;
     GP5_CATCH
 }
 
@@ -910,6 +933,11 @@ int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
     use_device(p);
     if (nsteps == 0) return GP5_OK;
     const bool merged = merged_path(p);
+    if (compensation_active(st) && st->comp_field != field) {
+        // the correction belongs to one state: a new state starts from zero
+        check_cuda(cudaMemsetAsync(st->comp, 0, p->field_bytes / 2 * (size_t)p->nsolve, p->stream), "memset");
+        st->comp_field = field;
+    }
     if (!st->exec || st->graph_field != field || st->graph_merged != merged || st->graph_steps != 1)
         build_graph(st, field, merged, 1);
     set_scalars(p->stream, st->ds, p->nsolve);
@@ -956,6 +984,7 @@ int gp5cu_stepper_advance_host(gp5cu_stepper *st, const void *host_in, void *hos
     use_device(p);
     if (!st->dstate) check_cuda(cudaMalloc(&st->dstate, p->field_bytes), "cudaMalloc state");
     check_cuda(cudaMemcpyAsync(st->dstate, host_in, p->field_bytes, cudaMemcpyHostToDevice, p->stream), "upload");
+    st->comp_field = nullptr;  // a new state: its correction starts from zero
     const int rc = gp5cu_stepper_advance(st, st->dstate, nsteps);
     if (rc != GP5_OK) return rc;
     check_cuda(cudaMemcpyAsync(host_out, st->dstate, p->field_bytes, cudaMemcpyDeviceToHost, p->stream), "download");

@@ -445,6 +445,7 @@ template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) 
         if (last) {
             P.phase_exp = (const V *)st->phase_exp;
             P.renorm_out = st->renorm ? 1 : 0;
+            if (compensation_active(st)) P.comp = (__nv_bfloat162 *)st->comp;
         }
         epilogue<Real>(p, P, last && st->renorm);
         launches += (p->ncomp == 1) ? 1 : 2;
@@ -498,6 +499,8 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
         P.turn = 1;
         P.renorm_out = st->renorm ? 1 : 0;
         P.phase_exp = nullptr;
+        P.comp = nullptr;
+        if (s == nst && compensation_active(st)) P.comp = (__nv_bfloat162 *)st->comp;
         if (!rk4) {
             P.mode = EPI_EULER;
             P.kprev = nullptr;

@@ -20,6 +20,8 @@
 // equal the host-side (and the reference's) values bit for bit.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "passes.cuh"
 
 namespace gp5 {
@@ -279,6 +281,9 @@ template <typename Real> struct EpiParams {
     const V *phase_exp;  // e^{i phi} or null
     // output renormalisation
     int renorm_out;
+    // compensated state (complex64 real-time runs): the part of psi below FP32 resolution,
+    // BF16 pairs; null = off.  psi1 = psi + (lo - d sum) is formed by a two-sum per lane
+    __nv_bfloat162 *comp;
 };
 
 template <typename Real>
@@ -363,7 +368,7 @@ __device__ __forceinline__ double interaction_energy(const EP &P, const SolvePar
 
 // Operands of one site's epilogue, loaded before any store of the batch.
 template <typename Real> struct EpiIn {
-    cpx<Real> psi, kprev, kacc;
+    cpx<Real> psi, kprev, kacc, lo;
 };
 
 template <typename Real>
@@ -372,6 +377,12 @@ __device__ __forceinline__ EpiIn<Real> epi_load(const EpiParams<Real> &P, long l
     in.psi = P.psi[g];
     in.kprev = P.mode >= EPI_RK2 ? P.kprev[g] : mk<Real>(0, 0);
     in.kacc = (P.mode == EPI_RK3 || P.mode == EPI_RK4) ? P.kacc[g] : mk<Real>(0, 0);
+    if (P.comp && (P.mode == EPI_RK4 || P.mode == EPI_EULER)) {
+        const float2 f = __bfloat1622float2(P.comp[g]);
+        in.lo = mk<Real>((Real)f.x, (Real)f.y);
+    } else {
+        in.lo = mk<Real>(0, 0);
+    }
     return in;
 }
 
@@ -469,7 +480,18 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
         const long long g = s + (long long)c * P.nsites;
         V sum = h[c];
         if (mode == EPI_RK4) sum = cadd(in[c].kacc, h[c]);
-        V r = csub(p[c], cmul(d, sum));
+        V r;
+        if (P.comp) {
+            // two-sum per lane: r + lo' = p + (lo - d sum) exactly when |p| >= |lo - d sum|
+            const V delta = csub(in[c].lo, cmul(d, sum));
+            r = cadd(p[c], delta);
+            V lo;
+            lo.x = (p[c].x - r.x) + delta.x;
+            lo.y = (p[c].y - r.y) + delta.y;
+            P.comp[g] = __floats2bfloat162_rn((float)lo.x, (float)lo.y);
+        } else {
+            r = csub(p[c], cmul(d, sum));
+        }
         if (P.phase_exp) {
             const Real a = sqrt(r.x * r.x + r.y * r.y);
             r = cscale(P.phase_exp[g], a);

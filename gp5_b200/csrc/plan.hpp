@@ -104,6 +104,11 @@ struct gp5cu_stepper {
     void *phase_exp = nullptr;  // e^{i phi}, plan precision, owned
     void *Ka = nullptr, *Kb = nullptr;
     void *dstate = nullptr;  // resident state of the host-buffer entry point
+    // compensated complex64 state (gp5cu_stepper_set_compensation): BF16 pairs per element, valid
+    // for the state at comp_field; active only without renormalisation and phase constraint
+    bool compensate = false;
+    void *comp = nullptr;
+    void *comp_field = nullptr;
     gp5::DevScalars *ds = nullptr;          // [nsolve]
     std::vector<gp5::SolveParams> sp_host;  // [nsolve]: functional + time step + targets
     gp5::SolveParams *sp = nullptr;
@@ -114,6 +119,11 @@ struct gp5cu_stepper {
     double t = 0;
     int launches_per_step = 0;
 };
+
+// the compensated update runs for complex64 plans without renormalisation or phase constraint
+inline bool compensation_active(const gp5cu_stepper *st) {
+    return st->compensate && st->comp && !st->renorm && !st->phase_exp && st->func->plan->prec == GP5_C64;
+}
 
 namespace gp5 {
 

@@ -14,6 +14,7 @@ No reference counterpart: the reference has no learned component.
 from __future__ import annotations
 
 import math
+import os
 from typing import Iterable, List, Optional, Sequence
 
 import numpy as np
@@ -21,7 +22,7 @@ import numpy as np
 from . import _abi
 
 N_SAMPLES = 64
-DEFAULT_WEIGHTS = __import__("os").path.join(__import__("os").path.dirname(__file__), "data", "warmstart_mlp.npz")
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_mlp.npz")
 OMEGAS = (0.0, 0.05, 0.1)
 C4 = 2.5
 
@@ -400,7 +401,6 @@ def evaluate(model: "WarmStart", count: int = 64, seed: int = TEST_SEED, n: int 
 def main(argv=None):
     import argparse
     import json
-    import os
     import time
 
     ap = argparse.ArgumentParser(description="Train or evaluate the droplet warm-start network.")

@@ -156,6 +156,13 @@ int gp5cu_stepper_set_renormalization(gp5cu_stepper *st, int n, const double *N)
  * dphase = real array (nx,ny,nz,ncomp) in the plan precision, device memory; NULL = the
  * nullConstraint (src/constraint.h:15-21). */
 int gp5cu_stepper_set_phase_constraint(gp5cu_stepper *st, const void *dphase);
+/* No reference counterpart.  Compensated state update for complex64 plans: the stepper keeps
+ * the part of psi below FP32 resolution in a BF16 pair per element and folds it into every
+ * step's update (two-sum), so increments far below the state's last bit are not lost (the
+ * source of complex64's norm and energy drift at small time steps).  Costs 8 bytes per site per
+ * step.  Active only without renormalisation and phase constraint; the correction restarts from
+ * zero when advance is given another state buffer (or a new host state).  on = 0 frees it. */
+int gp5cu_stepper_set_compensation(gp5cu_stepper *st, int on);
 /* timeStepper::advance(field, nSteps) (src/gpCpp.cpp:255-269): nsteps steps in place on a
  * device field; t += dt per step.  The step sequence is replayed from a CUDA graph. */
 int gp5cu_stepper_advance(gp5cu_stepper *st, void *dfield, int nsteps);
