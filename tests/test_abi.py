@@ -40,3 +40,21 @@ def test_argument_errors_without_device():
     assert rc == _abi.GP5_ERR_ARG
     rc = L.gp5cu_stepper_advance(None, None, 1)
     assert rc == _abi.GP5_ERR_ARG
+
+
+def test_every_declared_function_has_a_ctypes_prototype():
+    L = _abi.lib()
+    names = _abi.header_functions()
+    unbound = [n for n in names if getattr(L, n).argtypes is None]
+    assert not unbound, unbound
+
+
+def test_new_entry_points_reject_bad_arguments_without_device():
+    L = _abi.lib()
+    k = ctypes.c_int()
+    assert L.gp5cu_decompose(None, None, 0, 0.5, None, ctypes.byref(k)) == _abi.GP5_ERR_ARG
+    assert L.gp5cu_decompose_host(None, None, 0, 0.5, None, ctypes.byref(k)) == _abi.GP5_ERR_ARG
+    assert L.gp5cu_plan_get_tiles(None, None) == _abi.GP5_ERR_ARG
+    assert L.gp5cu_stepper_set_compensation(None, 1) == _abi.GP5_ERR_ARG
+    assert L.gp5cu_mlp_forward(None, None, 1, None) == _abi.GP5_ERR_ARG
+    assert L.gp5cu_gemm_bf16(None, 1, 1, None, 1, 1, None, 1, 1, 1, 1, None) == _abi.GP5_ERR_ARG
