@@ -224,8 +224,8 @@ int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps
         if (!g.st->exec || g.st->graph_field != g.psi || g.st->graph_steps != check_every)
             build_graph(g.st, g.psi, true, check_every);
     }
-    // round 0 checks the initial states; every later round advances check_every steps first
-    for (int round = 0;; round++) {
+    // check 0 looks at the initial states; every later check advances check_every steps first
+    for (int check = 0;; check++) {
         bool any = false;
         for (BatchGroup &g : b->groups) {
             gp5cu_plan *p = g.plan;
@@ -236,7 +236,7 @@ int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps
             any = true;
             dispatch_b(b->prec, [&](auto r) {
                 using Real = decltype(r);
-                if (round > 0) {
+                if (check > 0) {
                     set_scalars(p->stream, st->ds, p->nsolve);
                     Launch<Real>::prologue(st, g.psi);
                     check_cuda(cudaGraphLaunch(st->exec, p->stream), "cudaGraphLaunch");
@@ -263,7 +263,7 @@ int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps
                     act[q] = 0;
                     continue;
                 }
-                if (round > 0) steps[i] += check_every;
+                if (check > 0) steps[i] += check_every;
                 const DevScalars &d = g.ds_host[q];
                 const double dV = g.plan->sp_host[q].dV;
                 gp5cu_solve_result &R = results[i];

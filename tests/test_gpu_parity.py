@@ -1,7 +1,7 @@
 """GPU parity tests: the CUDA path, called through the C ABI, against the CPU oracle.
 
 Tolerances (relative to max |oracle|): complex128 transforms 1e-13, one RK4 step 1e-12
-1000 imaginary-time steps: psi 1e-10, E and mu 1e-10; complex64
+(the one-step target), 1000 imaginary-time steps: psi 1e-10, E and mu 1e-10; complex64
 transforms 2e-6.  The reference's own analytic tests keep their tolerances (1e-6, 1e-4).
 """
 import math
@@ -432,3 +432,24 @@ def test_nonfinite_is_reported(abi):
     with pytest.raises(abi.Gp5Error) as e:
         st.advance(a, 1)
     assert e.value.status == abi.GP5_ERR_NONFINITE
+
+
+def test_two_component_laplacian_reference_case(abi):
+    """tst/fft_test.cpp:156-215 (derivative_multipleComponents, a smoke test there): two
+    components, N = (200, 100, 100), box [-1,1]x[-1/2,1/2]^2, Gaussians of width 0.05 and
+    0.02; here checked against the analytic Laplacian of each component and the oracle."""
+    geo = o.Geometry((200, 100, 100), (-1.0, -0.5, -0.5), (1.0, 0.5, 0.5))
+    f = o.new_field(geo, 2)
+    o.init_gaussian(geo, 0.05, f, 0)
+    o.init_gaussian(geo, 0.02, f, 1)
+    p = make(abi, geo.shape, geo.left, geo.right, ncomp=2)
+    a, b = p.field(f), p.field()
+    p.laplacian(a, b)
+    got = b.download()
+    assert rel(got, o.laplacian(f, geo)) < 1e-12
+    X, Y, Z = o.grid(geo)
+    R2 = X * X + Y * Y + Z * Z
+    for c, s in ((0, 0.05), (1, 0.02)):
+        al = 1 / (2 * s * s)
+        ref = np.exp(-al * R2) * (-R2 * al * 2 + 3) * (-2) * al
+        assert np.max(np.abs(got[..., c].real - ref)) <= 1e-6 * np.max(np.abs(ref)), c
