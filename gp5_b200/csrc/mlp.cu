@@ -473,7 +473,7 @@ int gp5cu_mlp_create(gp5cu_mlp **out, int device, unsigned long long seed) {
     if (!out) return fail_m(GP5_ERR_ARG, "out is NULL");
     *out = nullptr;
     gp5cu_mlp *n = new gp5cu_mlp();
-    MLP_TRY
+    try {
     n->dev = device;
     ck(cudaSetDevice(device), "cudaSetDevice");
     ck(cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -507,7 +507,11 @@ int gp5cu_mlp_create(gp5cu_mlp **out, int device, unsigned long long seed) {
     refresh_bf16(n);
     ck(cudaStreamSynchronize(n->stream), "sync");
     *out = n;
-    MLP_CATCH
+    } catch (const std::string &e) {
+        gp5cu_mlp_destroy(n);  // frees whatever was allocated before the failure
+        return fail_m(GP5_ERR_CUDA, e);
+    }
+    return GP5_OK;
 }
 
 int gp5cu_mlp_destroy(gp5cu_mlp *n) {
@@ -621,30 +625,36 @@ int gp5cu_gemm_bf16(const void *A, long long sam, long long sak, const void *B, 
     MLP_TRY
     unsigned *err = nullptr;
     ck(cudaMalloc(&err, sizeof(unsigned)), "cudaMalloc");
-    ck(cudaMemsetAsync(err, 0, sizeof(unsigned), (cudaStream_t)stream), "memset");
-    GemmArgs a{};
-    a.A = (const bf16 *)A;
-    a.sam = sam;
-    a.sak = sak;
-    a.B = (const bf16 *)B;
-    a.sbn = sbn;
-    a.sbk = sbk;
-    a.M = M;
-    a.N = N;
-    a.K = K;
-    a.out32 = C;
-    a.ld = ldc;
-    a.err = err;
-    for (int n0 = 0; n0 < N; n0 += 256) {  // N tiles of 256 per launch group
-        GemmArgs b = a;
-        b.B = a.B + (long long)n0 * sbn;
-        b.N = N - n0 < 256 ? N - n0 : 256;
-        b.out32 = C + n0;
-        launch_gemm(b, (cudaStream_t)stream);
-    }
     unsigned e = 0;
-    ck(cudaMemcpyAsync(&e, err, sizeof(unsigned), cudaMemcpyDeviceToHost, (cudaStream_t)stream), "read err");
-    ck(cudaStreamSynchronize((cudaStream_t)stream), "sync");
+    try {
+        ck(cudaMemsetAsync(err, 0, sizeof(unsigned), (cudaStream_t)stream), "memset");
+        GemmArgs a{};
+        a.A = (const bf16 *)A;
+        a.sam = sam;
+        a.sak = sak;
+        a.B = (const bf16 *)B;
+        a.sbn = sbn;
+        a.sbk = sbk;
+        a.M = M;
+        a.N = N;
+        a.K = K;
+        a.out32 = C;
+        a.ld = ldc;
+        a.err = err;
+        for (int n0 = 0; n0 < N; n0 += 256) {  // N tiles of 256 per launch group
+            GemmArgs b = a;
+            b.B = a.B + (long long)n0 * sbn;
+            b.N = N - n0 < 256 ? N - n0 : 256;
+            b.out32 = C + n0;
+            launch_gemm(b, (cudaStream_t)stream);
+        }
+        ck(cudaMemcpyAsync(&e, err, sizeof(unsigned), cudaMemcpyDeviceToHost, (cudaStream_t)stream), "read err");
+        ck(cudaStreamSynchronize((cudaStream_t)stream), "sync");
+    } catch (...) {
+        cudaStreamSynchronize((cudaStream_t)stream);
+        cudaFree(err);  // the flag buffer is released on every path
+        throw;
+    }
     cudaFree(err);
     if (e) throw std::string("tensor-core GEMM: a bounded mbarrier wait ran out");
     MLP_CATCH
