@@ -73,3 +73,38 @@ def test_real_time_conserves_norm_and_energy_at_256cubed(setup, prec, tol_n, tol
     ob1 = f.observables(a)
     assert abs(ob1["norm"] / ob0["norm"] - 1) < tol_n
     assert abs(ob1["energy"] / ob0["energy"] - 1) < tol_e
+
+
+def test_config2_droplet_ground_state_then_real_time():
+    """The 128^3 LHY droplet (N = 500, L = 4 N^(1/3)): imaginary-time RK4 (dt = 5e-4,
+    renormalised) to a residual of 1e-10, then 2000 real-time RK4 steps (dt = 1e-4).  A
+    converged eigenstate only turns its phase in real time: |psi| stays put, the norm and the
+    energy are conserved and the phase turns at the rate mu."""
+    from gp5_b200 import _abi, warmstart as ws
+    N, n = 500.0, 128
+    L = ws.box_length(N)
+    p = _abi.Plan((n,) * 3, (-L / 2,) * 3, (L / 2,) * 3)
+    f = _abi.Functional(p, _abi.GP5_FUNC_LHY)
+    st = _abi.Stepper(f, 5e-4)
+    st.set_renormalization([N])
+    a = p.field(ws.gaussian_start(N, n, seed=2024)[..., None])
+    steps = 0
+    ob = f.observables(a)
+    while ob["residual"] > 1e-10 and steps < 400000:
+        st.advance(a, 5000)
+        steps += 5000
+        ob = f.observables(a)
+    assert ob["residual"] <= 1e-10, (steps, ob["residual"])
+    gs = a.download()
+    rt = _abi.Stepper(f, 1e-4, imaginary=False)
+    rt.advance(a, 2000)
+    ob2 = f.observables(a)
+    psi = a.download()
+    assert abs(ob2["norm"] / ob["norm"] - 1) < 1e-12
+    assert abs(ob2["energy"] / ob["energy"] - 1) < 1e-10
+    assert np.max(np.abs(np.abs(psi) - np.abs(gs))) <= 1e-7 * np.max(np.abs(gs))
+    # phase turned by -mu t at the droplet centre (psi ~ e^{-i mu t} psi0)
+    c = (n // 2, n // 2, n // 2, 0)
+    turn = np.angle(psi[c] / gs[c])
+    expected = -ob["mu"] * 2000 * 1e-4
+    assert abs((turn - expected + np.pi) % (2 * np.pi) - np.pi) < 1e-6
