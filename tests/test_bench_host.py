@@ -1,0 +1,46 @@
+"""bench.py's host-side arithmetic on CPU: the roofline figures of a step profile."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def merged_profile(ms):
+    """one RK4 step on the merged path: per stage y fwd (10), z (22), y inv (11), boundary (3)"""
+    out = []
+    for s in range(4):
+        out += [(10, ms["y"]), (22, ms["z"]), (11, ms["y"]), (3, ms["b"][s])]
+    return out
+
+
+def test_roofline_of_a_merged_step():
+    F = 256 ** 3 * 16
+    r = {"profile": merged_profile({"y": 0.1, "z": 0.12, "b": [0.25, 0.3, 0.35, 0.3]}), "field_bytes": F}
+    rf = bench.roofline(r, "c128")
+    assert rf["kernel"] == "x_stage_boundary" and rf["launches_per_step"] == 4
+    assert rf["algorithmic_bytes_per_launch"] == pytest.approx(5.75 * F)
+    # achieved = algorithmic bytes of the kind / its total time
+    assert rf["achieved"] == pytest.approx(23 * F / 1.2e-3 / 1e9, rel=1e-3)
+    step = rf["step"]
+    assert step["algorithmic_bytes"] == 47 * F and step["bytes_per_site"] == 752.0
+    assert step["achieved"] == pytest.approx(47 * F / (4 * (0.1 + 0.12 + 0.1) + 1.2) / 1e6, rel=1e-3)
+    peak, src = bench.measured_peaks()
+    assert rf["peak"] == peak and rf["frac"] == pytest.approx(rf["achieved"] / peak, abs=1e-4)
+    assert rf["share_of_step"] == pytest.approx(1.2 / (4 * 0.32 + 1.2), abs=1e-4)
+
+
+def test_roofline_traffic_comes_from_the_matching_precision():
+    F = 256 ** 3 * 16
+    r = {"profile": merged_profile({"y": 0.1, "z": 0.12, "b": [0.3] * 4}), "field_bytes": F}
+    t128 = bench.roofline(r, "c128")["traffic"]
+    t64 = bench.roofline(dict(r, field_bytes=F // 2), "c64")["traffic"]
+    assert t128 is None or t128 > 5 * F  # committed ncu summary of the complex128 boundary
+    assert t64 is None  # no complex64 capture is committed
+
+
+def test_unknown_profiles_give_no_roofline():
+    assert bench.roofline({"profile": [(3, 1.0)] * 7, "field_bytes": 16}) is None

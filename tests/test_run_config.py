@@ -1,5 +1,6 @@
 """The YAML front end (gp5_b200/run.py): configuration parsing and host-side arrays on CPU."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -76,3 +77,71 @@ def test_potential_sum_and_files(tmp_path):
     assert np.array_equal(back, extra) and back.flags["F_CONTIGUOUS"]
     with pytest.raises(R.ConfigError, match="h5py"):
         R.read_array(str(tmp_path / "x.hdf5"))
+
+
+class _FakeField:
+    def __init__(self, plan, host=None):
+        self.plan = plan
+        self.a = np.zeros(plan.field_shape, complex) if host is None else np.array(host, complex)
+        self.ptr = type("P", (), {"value": 0})()
+
+    def download(self):
+        return self.a.copy()
+
+    def upload(self, host):
+        self.a = np.array(host, complex)
+
+
+class _FakePlan:
+    def __init__(self, shape, left, right, ncomp=1, precision=0, device=0):
+        self.field_shape = tuple(shape) + (ncomp,)
+        self.precision = precision
+        self.h = None
+
+    def field(self, host=None):
+        return _FakeField(self, host)
+
+
+class _FakeFunctional:
+    def __init__(self, plan, kind, **kw):
+        self.kw = kw
+
+
+class _FakeStepper:
+    calls = []
+
+    def __init__(self, func, dt, kind, imaginary=True):
+        self.dt = dt
+
+    def set_renormalization(self, N):
+        pass
+
+    def set_phase_constraint(self, p):
+        pass
+
+    def advance(self, f, n):
+        _FakeStepper.calls.append(n)
+        f.a = f.a + n  # a trace of the steps taken
+
+
+@pytest.mark.parametrize("max_time", [0.015, 0.02, 0.0])
+def test_run_loop_outputs_and_time(tmp_path, monkeypatch, max_time):
+    monkeypatch.setattr(R._abi, "Plan", _FakePlan)
+    monkeypatch.setattr(R._abi, "Functional", _FakeFunctional)
+    monkeypatch.setattr(R._abi, "Stepper", _FakeStepper)
+    _FakeStepper.calls = []
+    c = base_cfg()
+    c["evolution"]["maxTime"] = max_time
+    np.save(tmp_path / "init.npy", np.zeros((24, 20, 16, 1), complex))
+    r = R.run(c, base=str(tmp_path), log=lambda *_: None)
+    # the reference's loop: while t <= maxTime { save; nIterations x (advance; t += dt) }
+    t, k = 0.0, 0
+    while t <= max_time:
+        for _ in range(10):
+            t += 1e-3
+        k += 1
+    assert len(r["files"]) == k and r["steps"] == 10 * k and r["time"] == t
+    assert _FakeStepper.calls == [10] * k
+    for j, fpath in enumerate(r["files"]):
+        assert fpath.endswith(f"out_{j}.npy") and os.path.dirname(fpath) == str(tmp_path / "out")
+        assert np.all(np.load(fpath) == 10 * j)  # out_j is saved before block j advances
