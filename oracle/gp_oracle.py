@@ -34,6 +34,49 @@ except Exception:  # pragma: no cover
 
 _WORKERS = int(os.environ.get("GP5_ORACLE_WORKERS", "0")) or (os.cpu_count() or 1)
 
+# Element-wise work (the K^2 multiply, the functional's point-wise terms, the RK stage
+# combinations) can run over z-slabs on a thread pool: numpy releases the GIL inside its
+# loops, and every element goes through the same expression as in the serial form.
+# Reductions (norms) stay serial.  Default: one thread (the tests' setting).
+_EW_THREADS = 1
+_EW_POOL = None
+
+
+def set_elementwise_threads(n: int) -> None:
+    global _EW_THREADS, _EW_POOL
+    n = max(1, int(n))
+    if n > 1 and (_EW_POOL is None or _EW_THREADS != n):
+        from concurrent.futures import ThreadPoolExecutor
+        _EW_POOL = ThreadPoolExecutor(max_workers=n)
+    _EW_THREADS = n
+
+
+def _slabs(fn, *arrays, min_size: int = 1 << 16):
+    """fn(*arrays) for element-wise fn; with more than one thread, evaluated slab by slab
+    along axis 2 (arrays of 3 or more dimensions are sliced, anything else is passed as is)."""
+    first = next((a for a in arrays if isinstance(a, np.ndarray) and a.ndim >= 3), None)
+    if _EW_THREADS <= 1 or first is None or first.size < min_size or first.shape[2] < 2:
+        return fn(*arrays)
+    nz = first.shape[2]
+    nt = min(_EW_THREADS, nz)
+    b = np.linspace(0, nz, nt + 1).astype(int)
+
+    def cut(a, i):
+        return a[:, :, b[i]:b[i + 1]] if isinstance(a, np.ndarray) and a.ndim >= 3 else a
+
+    parts = list(_EW_POOL.map(lambda i: fn(*[cut(a, i) for a in arrays]), range(nt)))
+    # the serial expression keeps its first operand's layout; so does this (a transform of the
+    # result rounds differently on a differently laid out array)
+    order = "F" if first.flags.f_contiguous and not first.flags.c_contiguous else "C"
+    out = np.empty(parts[0].shape[:2] + (nz,) + parts[0].shape[3:], dtype=parts[0].dtype, order=order)
+
+    def put(i):
+        out[:, :, b[i]:b[i + 1]] = parts[i]
+
+    list(_EW_POOL.map(put, range(nt)))
+    return out
+
+
 
 # --------------------------------------------------------------------------------------
 # geometry (src/geometry.h, src/geometry.cpp)
@@ -174,9 +217,10 @@ def laplacian(psi: np.ndarray, geo: Geometry) -> np.ndarray:
     """dst = IFFT(-K^2 * FFT(src)) * (1/N^3) (laplacian::apply, operators.cpp:28-36)."""
     K2 = k2_tensor(geo)[..., None]
     fk = fft3(psi, FORWARD)
-    fk = -fk * K2
+    fk = _slabs(lambda f, k: -f * k, fk, K2)
     out = fft3(fk, BACKWARD)
-    return out * (1.0 / complex(geo.n_sites, 0))
+    scale = 1.0 / complex(geo.n_sites, 0)
+    return _slabs(lambda o: o * scale, out)
 
 
 # --------------------------------------------------------------------------------------
@@ -226,9 +270,11 @@ class Functional:
 
     def kinetic(self, psi: np.ndarray, geo: Geometry) -> np.ndarray:
         """-1/2 (1/m) lap(psi) as the reference forms it (before potential/interaction)."""
-        lap = laplacian(psi, geo)
+        return self._kinetic_of(laplacian(psi, geo))
+
+    def _kinetic_of(self, lap: np.ndarray) -> np.ndarray:
         if self.kind == "gp":
-            ncomp = psi.shape[3]
+            ncomp = lap.shape[3]
             masses = list(self.masses) if self.masses is not None else [1.0] * ncomp
             out = np.empty_like(lap)
             for c in range(ncomp):
@@ -268,17 +314,20 @@ class Functional:
 
     def apply(self, psi: np.ndarray, geo: Geometry) -> np.ndarray:
         """H psi in the reference's order: kinetic, (+ V psi), + f psi."""
-        out = self.kinetic(psi, geo)
+        return _slabs(self._apply_tail, laplacian(psi, geo), psi, self.V)
+
+    def _apply_tail(self, lap: np.ndarray, psi: np.ndarray, V) -> np.ndarray:
+        out = self._kinetic_of(lap)
         if self.kind == "gp":
             # gpFunctional::apply: kinetic, addPotential, then mean field (functional.cpp:13-43)
-            if self.V is not None:
-                out = out + self.V * psi
+            if V is not None:
+                out = out + V * psi
             out = out + self.interaction_factor(psi) * psi
         else:
             # LHY: kinetic + f psi in one expression, then addPotential (functional.cpp:112-121)
             out = out + self.interaction_factor(psi) * psi
-            if self.V is not None:
-                out = out + self.V * psi
+            if V is not None:
+                out = out + V * psi
         return out
 
     # ---- energy density pieces (no reference counterpart; project definitions) -------
@@ -357,28 +406,28 @@ class Stepper:
     def _constrain(self, f: np.ndarray) -> np.ndarray:
         if self.constraint_phase is None:
             return f
-        return np.sqrt(f * np.conj(f)) * np.exp(1j * self.constraint_phase)
+        return _slabs(lambda a, ph: np.sqrt(a * np.conj(a)) * np.exp(1j * ph), f, self.constraint_phase)
 
     def step(self, psi0: np.ndarray) -> np.ndarray:
         tau = self.tau
         H = lambda u: self.func.apply(u, self.geo)  # noqa: E731
         if self.name.lower() in ("eulero", "euler"):
             k1 = H(psi0)
-            new = psi0 - tau * k1
+            new = _slabs(lambda a, k: a - tau * k, psi0, k1)
             new = self._constrain(new)
             self._normalize(new)
             return new
         k1 = H(psi0)
-        new = psi0 - tau * 0.5 * k1
+        new = _slabs(lambda a, k: a - tau * 0.5 * k, psi0, k1)
         self._normalize(new)
         k2 = H(new)
-        new = psi0 - tau * 0.5 * k2
+        new = _slabs(lambda a, k: a - tau * 0.5 * k, psi0, k2)
         self._normalize(new)
         k3 = H(new)
-        new = psi0 - tau * k3
+        new = _slabs(lambda a, k: a - tau * k, psi0, k3)
         self._normalize(new)
         k4 = H(new)
-        new = psi0 - (1.0 / 6) * tau * (k1 + 2 * k2 + 2 * k3 + k4)
+        new = _slabs(lambda a, b, c, d, e: a - (1.0 / 6) * tau * (b + 2 * c + 2 * d + e), psi0, k1, k2, k3, k4)
         new = self._constrain(new)
         self._normalize(new)
         return new

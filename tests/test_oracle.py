@@ -172,3 +172,28 @@ def test_decompose_periodic_diagonal_order_and_cutoff():
     assert lab[0, 3, 3, 0] == lab[11, 3, 3, 0] == 1
     assert lab[2, 0, 0, 0] == 2 and lab[5, 5, 5, 0] == lab[6, 6, 6, 0] == 3
     assert lab[8, 9, 7, 0] == -1 and (lab[..., 1] == 0).all()
+
+
+def test_threaded_elementwise_oracle_is_bitwise_serial():
+    """set_elementwise_threads only spreads the element-wise expressions over z-slabs: the
+    results must not change by a bit."""
+    geo = o.Geometry((48, 40, 36), (-6,) * 3, (6,) * 3)
+    psi = o.gaussian_with_noise(geo, 1.5, 1e-3, seed=5, N=40.0, phase_noise=True)
+    psi2 = np.concatenate([psi, 0.5 * psi], axis=3)
+    V = np.asfortranarray(np.random.default_rng(1).uniform(0, 1, psi.shape))
+    phase = np.asfortranarray(np.random.default_rng(2).uniform(-3, 3, psi.shape))
+    cases = [
+        lambda: o.Stepper(o.Functional("lhy", c3=-3.3, V=V), geo, 1e-3, imaginary=False).advance(psi.copy(), 2),
+        lambda: o.Stepper(o.Functional("gp", couplings=np.array([[1.0, 0.3], [0.3, 2.0]]), masses=[1.0, 2.0]),
+                          geo, 1e-3, normalizations=[40.0, 10.0]).advance(psi2.copy(), 2),
+        lambda: o.Stepper(o.Functional("lhy"), geo, 1e-3, "eulero", False,
+                          constraint_phase=phase).advance(psi.copy(), 2),
+    ]
+    try:
+        serial = [c() for c in cases]
+        o.set_elementwise_threads(4)
+        threaded = [c() for c in cases]
+    finally:
+        o.set_elementwise_threads(1)
+    for a, b in zip(serial, threaded):
+        assert np.array_equal(a, b)
