@@ -107,3 +107,30 @@ def test_image_sum_placement_reproduces_periodic_droplet():
     assert err < 2e-3 and err < 0.2 * err_radial, (err, err_radial)
     assert got.flags["F_CONTIGUOUS"] and got.dtype == np.complex128
     assert abs(np.sum(np.abs(got) ** 2) * (L / n) ** 3 - N) < 1e-9 * N
+
+
+def test_free_profile_recovers_the_isolated_profile():
+    """Axis samples of a periodic image sum of a known isolated profile (smooth core, screened-
+    Coulomb tail) deconvolve back to that profile and its tail rate."""
+    N, kappa = 60.0, 0.7
+    r = ws.radii(N)
+    R, L = r[-1], ws.box_length(N)
+    rc = 0.25 * R  # the tail dominates the last samples, as for a droplet
+
+    def f(d):
+        d = np.asarray(d, float)
+        core = np.exp(-(d / rc) ** 2)
+        tail = 0.03 * np.exp(-kappa * d) / np.maximum(d, 1e-12)
+        w = 1 - np.exp(-(d / rc) ** 6)
+        return core + w * tail
+
+    # the isolated profile seen through the front end's tail model beyond R
+    samples_iso = f(r)
+    axis = np.zeros_like(r)
+    for m in ws._AXIS_IMAGES:
+        d = np.sqrt((r - m[0] * L) ** 2 + (m[1] * L) ** 2 + (m[2] * L) ** 2)
+        axis += np.where(d <= R, f(np.minimum(d, R)),
+                         f(R) * (R / np.maximum(d, R)) * np.exp(-kappa * (np.maximum(d, R) - R)))
+    got, k = ws.free_profile(axis, N)
+    assert 0.5 * kappa < k < 1.5 * kappa  # log-slope estimate (the core still leaks into it)
+    assert np.max(np.abs(got - samples_iso)) < 1e-5 * np.max(samples_iso)
