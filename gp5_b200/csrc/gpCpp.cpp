@@ -256,6 +256,13 @@ public:
         check(gp5cu_stepper_set_time(_st, t));
         _plan = m.plan();
         if (!_norms.empty()) check(gp5cu_stepper_set_renormalization(_st, (int)_norms.size(), _norms.data()));
+        if (_compensate) check(gp5cu_stepper_set_compensation(_st, 1));
+    }
+    // extension (no reference counterpart): compensated complex64 state update, see
+    // gp5cu_stepper_set_compensation; kept across setFunctional
+    void setCompensation(bool on) {
+        _compensate = on;
+        if (_st) check(gp5cu_stepper_set_compensation(_st, on ? 1 : 0));
     }
     void setRenormalization(const std::vector<double> &normalizations) {
         _norms = normalizations;
@@ -284,6 +291,7 @@ private:
     gp5cu_stepper *_st = nullptr;
     gp5cu_plan *_plan = nullptr;
     std::vector<double> _norms;
+    bool _compensate = false;
 };
 
 }  // namespace
@@ -324,6 +332,7 @@ PYBIND11_MODULE(gpCpp, m) {
     py::class_<timeStepper>(m, "timeStepper")
         .def(py::init<double, std::string, bool>())
         .def("setRenormalization", &timeStepper::setRenormalization)
+        .def("setCompensation", &timeStepper::setCompensation)
         .def("unsetRenormalization", &timeStepper::unsetRenormalization)
         .def("setFunctional", &timeStepper::setFunctional)
         .def("advance", &timeStepper::advance)

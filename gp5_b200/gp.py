@@ -189,8 +189,9 @@ class GP(_model):
 
 
 class stepper:
-    def __init__(self, model, timeStep, name="RK4", imaginary=True, renormalize=False):
-        """name: str, allowed: RK4, eulero"""
+    def __init__(self, model, timeStep, name="RK4", imaginary=True, renormalize=False, compensate=False):
+        """name: str, allowed: RK4, eulero.  compensate (extension): compensated state update for
+        complex64 fields (the part of psi below FP32 resolution is carried between steps)."""
         self._timeStep = timeStep
         self._name = name
         self._imaginary = imaginary
@@ -199,6 +200,11 @@ class stepper:
         self._stepperCpp.setFunctional(model._funcCpp)
         self._renormalize = False
         self._stepperCpp.unsetRenormalization()
+        if compensate:
+            self._stepperCpp.setCompensation(True)
+
+    def setCompensation(self, on):
+        self._stepperCpp.setCompensation(bool(on))
 
     def setRenormalization(self, N):
         self._stepperCpp.setRenormalization(list(N))

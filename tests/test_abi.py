@@ -58,3 +58,12 @@ def test_new_entry_points_reject_bad_arguments_without_device():
     assert L.gp5cu_stepper_set_compensation(None, 1) == _abi.GP5_ERR_ARG
     assert L.gp5cu_mlp_forward(None, None, 1, None) == _abi.GP5_ERR_ARG
     assert L.gp5cu_gemm_bf16(None, 1, 1, None, 1, 1, None, 1, 1, 1, 1, None) == _abi.GP5_ERR_ARG
+
+
+def test_reference_facing_bindings_expose_the_extensions():
+    import inspect
+
+    from gp5_b200 import gp, gpCpp
+    assert hasattr(gpCpp.timeStepper, "setCompensation") and hasattr(gpCpp, "decomposition")
+    assert "compensate" in inspect.signature(gp.stepper.__init__).parameters
+    assert hasattr(gp.stepper, "setCompensation")
