@@ -1,6 +1,7 @@
 """CPU checks of the C ABI library: it loads, exports every function include/gp5cu.h
 declares, and reports errors as status codes (no device work is attempted here)."""
 import ctypes
+import os
 
 from gp5_b200 import _abi
 
@@ -67,3 +68,53 @@ def test_reference_facing_bindings_expose_the_extensions():
     assert hasattr(gpCpp.timeStepper, "setCompensation") and hasattr(gpCpp, "decomposition")
     assert "compensate" in inspect.signature(gp.stepper.__init__).parameters
     assert hasattr(gp.stepper, "setCompensation")
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/gp5cu.h compiles as C99 and a C caller links against libgp5cu.so (no run: the
+    program would need a GPU)."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        import pytest
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "caller.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "gp5cu.h"
+int main(void) {
+    gp5cu_plan *plan = NULL;
+    const int shape[3] = {64, 64, 64};
+    const double left[3] = {-10, -10, -10}, right[3] = {10, 10, 10};
+    if (gp5cu_plan_create(&plan, shape, left, right, 1, GP5_C128, 0) != GP5_OK) {
+        fprintf(stderr, "%s\n", gp5cu_last_error());
+        return 1;
+    }
+    gp5cu_functional_desc d;
+    gp5cu_functional_desc_init(&d);
+    d.kind = GP5_FUNC_GP; d.has_couplings = 1; d.couplings[0] = 1.0;
+    d.potential = GP5_POT_HARMONIC; d.omegas[0][0] = d.omegas[0][1] = d.omegas[0][2] = 1.0;
+    gp5cu_functional *f = NULL;
+    gp5cu_stepper *st = NULL;
+    void *psi = NULL;
+    gp5cu_functional_create(plan, &d, &f);
+    gp5cu_stepper_create(f, GP5_STEP_RK4, 1e-3, 1, &st);
+    gp5cu_field_alloc(plan, &psi);
+    gp5cu_stepper_advance(st, psi, 10);
+    gp5cu_observables_t ob;
+    gp5cu_observables(f, psi, &ob);
+    printf("E = %g\n", ob.energy);
+    gp5cu_field_free(plan, psi);
+    gp5cu_stepper_destroy(st);
+    gp5cu_functional_destroy(f);
+    return gp5cu_plan_destroy(plan);
+}
+''')
+    lib = os.path.join(root, "gp5_b200")
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(root, "include"), str(src),
+                        "-L", lib, "-lgp5cu", "-Wl,-rpath," + lib, "-o", str(tmp_path / "caller")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
