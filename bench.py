@@ -178,6 +178,32 @@ def sum_over_ranks(x: float, world: int) -> float:
     return _reduce(x, world, "sum")
 
 
+def timed_repeats(run, stream, world: int, min_seconds: float):
+    """Times `run` (exactly K steps) with CUDA events on `stream`, each repeat bracketed by a
+    barrier and a device synchronisation on both sides, the max over ranks per repeat; repeats
+    until `min_seconds` of timed work have passed (every rank runs the same count), so that the
+    clock sampler sees the timed region.  Returns the per-repeat milliseconds."""
+    import torch
+
+    out = []
+    reps = None
+    while reps is None or len(out) < reps:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        out.append(ms)
+        if reps is None:
+            # one count for all ranks (ms is already the max over ranks)
+            reps = max(1, min(1000, int(math.ceil(min_seconds * 1e3 / max(ms, 1e-3)))))
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -202,21 +228,15 @@ def run_ours(args, rank, world, local_rank):
         f = plan.field(psi0)
         st.advance(f, args.warmup)  # builds the step graph; W untimed steps
         with torch.cuda.stream(stream):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            if world > 1:
-                torch.distributed.barrier()
             with ClockSampler(dev) as clk:
                 time.sleep(1.0)  # nvidia-smi is sampling before the timed region starts
-                e0.record(stream)
-                st.advance(f, args.steps)
-                e1.record(stream)
-                torch.cuda.synchronize()
-            ms = max_over_ranks(e0.elapsed_time(e1), world)
+                reps_ms = timed_repeats(lambda: st.advance(f, args.steps), stream, world, args.min_seconds)
+            ms = statistics.median(reps_ms)
         lps = st.launches_per_step
-        launches += lps * args.steps + 1  # + the prologue transform of each advance call
+        launches += (lps * args.steps + 1) * len(reps_ms)  # + the prologue transform of each advance call
         r = {"ms": ms, "ms_per_step": ms / args.steps, "value": world * sites * args.steps / (ms / 1e3),
-             "clocks": clk.summary(), "launches_per_step": lps, "tiles": plan.tiles()}
+             "clocks": clk.summary(), "launches_per_step": lps, "tiles": plan.tiles(),
+             "repeats": len(reps_ms), "ms_per_step_spread": [min(reps_ms) / args.steps, max(reps_ms) / args.steps]}
         # per-launch durations of one step (CUDA events between launches, same stream)
         prof = st.profile(f, nrep=3)
         r["profile"] = prof
@@ -373,6 +393,52 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
                         "quench to c3=-3.3, real-time RK4 dt=5e-5"}
 
 
+def precision_check(dev: int, steps: int = 500, every: int = 100):
+    """complex64 (plain and compensated) against complex128 on the bench workload itself: the
+    same initial state, `steps` real-time RK4 steps of the quenched droplet in each precision;
+    every `every` steps the norm and the energy (FP64 reductions, complex64 state evaluated by
+    the complex128 functional) against the complex128 run.  Returns the maxima."""
+    import numpy as np
+
+    from gp5_b200 import _abi
+
+    shape, left, right = workload_geometry()
+    psi0 = initial_state()
+    p64 = _abi.Plan(shape, left, right, precision=_abi.GP5_C128, device=dev)
+    p32 = _abi.Plan(shape, left, right, precision=_abi.GP5_C64, device=dev)
+    f_eval = _abi.Functional(p64, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
+    e_field = p64.field()
+    rows = {}
+    for name, p, comp in (("c128", p64, False), ("c64", p32, False), ("c64c", p32, True)):
+        fq = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
+        sq = _abi.Stepper(fq, DT, _abi.GP5_STEP_RK4, imaginary=False)
+        if comp:
+            sq.set_compensation(True)
+        g = p.field(psi0)
+        out = []
+        for k in range(0, steps + 1, every):
+            if k:
+                sq.advance(g, every)
+            if p is p64:
+                o = f_eval.observables(g)
+            else:
+                e_field.upload(np.asarray(g.download(), dtype=np.complex128))
+                o = f_eval.observables(e_field)
+            out.append((o["norm"], o["energy"]))
+        rows[name] = out
+        del g, sq, fq
+    ref = rows["c128"]
+    n0 = ref[0][0]
+    res = {"steps": steps, "every": every,
+           "max_norm_drift_c128": max(abs(n - n0) / n0 for n, _ in ref)}
+    for name in ("c64", "c64c"):
+        res["max_energy_rel_err_" + name] = max(abs(e - er) / abs(er) for (_, e), (_, er) in zip(rows[name], ref))
+        res["max_norm_drift_" + name] = max(abs(n - n0) / n0 for n, _ in rows[name])
+    res["workload"] = ("bench workload (Gaussian start, c3=-3.3), real-time RK4 dt=5e-5 in each precision "
+                       "from the same state; complex64 states evaluated in complex128")
+    return res
+
+
 # ---- batched droplet ground states (config: 64 seeded solves; bench leg: a seeded sample) ----
 def batch_solves(count: int, seed: int = 2025, rank: int = 0):
     """N log-uniform in [20, 2000], c3 ~ U[-3.2, -2.8], c4 = 2.5, no trap, L = 4 N^(1/3); grid:
@@ -407,13 +473,14 @@ def droplet_state(sd, seed):
     return np.asfortranarray(psi)
 
 
-def run_batch(count: int, dev: int, tol: float = 1e-8, rank: int = 0, world: int = 1):
+def run_batch(count: int, dev: int, tol: float = 1e-8, rank: int = 0, world: int = 1, precision: str = "c128"):
     import torch
 
     from gp5_b200 import _abi
 
     solves = batch_solves(count, rank=rank)
-    b = _abi.Batch(solves, precision=_abi.GP5_C128, device=dev)
+    prec = _abi.GP5_C128 if precision == "c128" else _abi.GP5_C64
+    b = _abi.Batch(solves, precision=prec, device=dev)
     for k, sd in enumerate(solves):
         b.set_state(k, droplet_state(sd, 3000 + 1000 * rank + k))
     torch.cuda.synchronize()
@@ -428,19 +495,61 @@ def run_batch(count: int, dev: int, tol: float = 1e-8, rank: int = 0, world: int
     grids = {}
     for sd in solves:
         grids[str(sd["n"])] = grids.get(str(sd["n"]), 0) + 1
-    return {"value": conv / wall, "unit": "ground states/s", "solves": count * world, "converged": conv,
-            "tol": tol, "seconds": wall, "dtype": "c128", "grids_rank0": grids,
-            "steps_rank0": {"min": min(r["steps"] for r in res), "max": max(r["steps"] for r in res),
-                            "mean": sum(r["steps"] for r in res) / count},
-            "site_updates_per_s": site_steps / wall, "gpu_launches": launches,
-            "workload": "seeded LHY droplets (one shard of " + str(count) + " per rank): N log-uniform "
-                        "[20,2000], c3 U[-3.2,-2.8], c4 2.5, Gaussian start (width 0.5 N^(1/3), phase "
-                        "noise 1e-3), imaginary-time RK4 renormalised every step, dt 0.15 dx^2, residual "
-                        "checked every 500 steps"}
+    out = {"value": conv / wall, "unit": "ground states/s", "solves": count * world, "converged": conv,
+           "tol": tol, "seconds": wall, "dtype": precision, "grids_rank0": grids,
+           "steps_rank0": {"min": min(r["steps"] for r in res), "max": max(r["steps"] for r in res),
+                           "mean": sum(r["steps"] for r in res) / count},
+           "site_updates_per_s": site_steps / wall, "gpu_launches": launches,
+           "energies_rank0": [r["energy"] for r in res],
+           "workload": "seeded LHY droplets (one shard of " + str(count) + " per rank): N log-uniform "
+                       "[20,2000], c3 U[-3.2,-2.8], c4 2.5, Gaussian start (width 0.5 N^(1/3), phase "
+                       "noise 1e-3), imaginary-time RK4 renormalised every step, dt 0.15 dx^2, residual "
+                       "checked every 500 steps"}
+    if precision == "c64":
+        out["steps_c64_rank0_mean"] = sum(r["steps_c64"] for r in res) / count
+        out["method"] = ("complex64 state and transforms (FP64 reductions) until the residual reaches 1e-5 "
+                         "or stops falling, then complex128 to the tolerance")
+    out["_steps"] = [r["steps"] for r in res]
+    out["_grids"] = [sd["n"] for sd in solves]
+    return out
 
 
-def cpu_reference_timing(max_seconds: float, max_steps: int, warm: bool = True):
-    """RK4 steps of the oracle (the reference's arithmetic) on the host, all threads."""
+def cpu_ground_state_baseline(gs: dict, seconds_per_grid: float = 4.0):
+    """Ground states/s of the oracle (the reference's arithmetic: renormalised imaginary-time
+    RK4, all host threads) on the same seeded droplets, extrapolated: for every grid size of the
+    batch, the time of one oracle RK4 step is measured on a bounded sample of steps of a
+    droplet of that grid, and each solve is charged the steps the GPU solver needed for it
+    (the same algorithm in the same arithmetic takes the same steps)."""
+    import numpy as np
+
+    from oracle import gp_oracle as o
+
+    o.set_elementwise_threads(o._WORKERS)
+    per_step = {}
+    sample = []
+    for n in sorted(set(gs["_grids"])):
+        sd = next(s for s in batch_solves(len(gs["_grids"])) if s["n"] == n)
+        geo = o.Geometry((n,) * 3, (-sd["L"] / 2,) * 3, (sd["L"] / 2,) * 3)
+        psi = np.asfortranarray(droplet_state(sd, 1)[..., None])
+        st = o.Stepper(o.Functional("lhy", c3=sd["c3"], c4=sd["c4"]), geo, sd["dt"], "RK4", imaginary=True,
+                       normalizations=[sd["N"]])
+        psi = st.advance(psi, 1)  # warm
+        k, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < seconds_per_grid or k < 2:
+            psi = st.advance(psi, 1)
+            k += 1
+        per_step[n] = (time.perf_counter() - t0) / k
+        sample.append(f"{k} RK4 steps at {n}^3")
+    total = sum(steps * per_step[n] for steps, n in zip(gs["_steps"], gs["_grids"]))
+    return {"value": len(gs["_steps"]) / total, "unit": "ground states/s", "cores": o._WORKERS, "kind": "port",
+            "seconds_per_step": {str(n): t for n, t in per_step.items()},
+            "sample": "; ".join(sample) + "; extrapolated to the GPU solver's step count of every solve "
+                      f"({sum(gs['_steps'])} steps in total, {total:.0f} s on the host)"}
+
+
+def cpu_reference_timing(max_seconds: float, max_steps: int, warmup: int = 1):
+    """RK4 steps of the oracle (the reference's arithmetic) on the host, all threads: `warmup`
+    untimed steps, then up to `max_steps` timed steps or `max_seconds`, whichever ends first."""
     from oracle import gp_oracle as o
 
     shape, left, right = workload_geometry()
@@ -450,8 +559,8 @@ def cpu_reference_timing(max_seconds: float, max_steps: int, warm: bool = True):
     # z-slabs (the reference spreads both over its MPI ranks)
     o.set_elementwise_threads(o._WORKERS)
     st = o.Stepper(o.Functional("lhy", c3=C3, c4=C4), geo, DT, "RK4", imaginary=False)
-    if warm:
-        psi = st.advance(psi, 1)
+    if warmup > 0:
+        psi = st.advance(psi, warmup)
     n, t0 = 0, time.perf_counter()
     while n < max_steps:
         psi = st.advance(psi, 1)
@@ -460,7 +569,7 @@ def cpu_reference_timing(max_seconds: float, max_steps: int, warm: bool = True):
             break
     dt = time.perf_counter() - t0
     return {"value": N_GRID ** 3 * n / dt, "unit": "site-updates/s", "cores": o._WORKERS, "kind": "port",
-            "steps": n, "seconds": dt,
+            "steps": n, "seconds": dt, "warmup": warmup,
             "sample": f"{n} RK4 step(s) of the 256^3 complex128 workload; scipy.fft with "
                       f"{o._WORKERS} workers, element-wise numpy over {o._WORKERS} threads"}
 
@@ -472,10 +581,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--min-seconds", type=float, default=2.0,
+                    help="repeat the timed K steps until this much timed work has passed (clock sampling)")
     ap.add_argument("--precision-report", metavar="JSON",
                     help="also run the complex64-vs-complex128 quench report and write it here")
-    ap.add_argument("--batch", type=int, default=16,
-                    help="solves of the ground-state leg (0: skip; the full configuration is 64)")
+    ap.add_argument("--batch", type=int, default=64,
+                    help="solves of the ground-state leg, in complex128 and in complex64 (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -491,11 +602,12 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        budget = 150.0
-        r = cpu_reference_timing(max_seconds=budget / max(1, args.steps) * args.steps, max_steps=args.steps,
-                                 warm=True)
+        # a bounded sample: at most ~150 s of timed CPU steps (one step of the oracle at 256^3
+        # takes about a second on 16 host threads)
+        r = cpu_reference_timing(max_seconds=150.0, max_steps=args.steps, warmup=args.warmup)
         line = {"impl": "reference", "metric": metric, "value": r["value"], "unit": "site-updates/s",
-                "n_gpus": args.gpus, "steps": r["steps"], "warmup": 1, "ms_per_step": r["seconds"] / r["steps"] * 1e3,
+                "n_gpus": args.gpus, "steps": r["steps"], "warmup": r["warmup"],
+                "ms_per_step": r["seconds"] / r["steps"] * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
@@ -512,7 +624,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device(f"cuda:{local_rank}"))
     results, launches = run_ours(args, rank, world, local_rank)
-    gs = run_batch(args.batch, local_rank, rank=rank, world=world) if args.batch > 0 else None
+    gs = None
+    if args.batch > 0:
+        gs = run_batch(args.batch, local_rank, rank=rank, world=world, precision="c128")
+        gs["c64"] = run_batch(args.batch, local_rank, rank=rank, world=world, precision="c64")
     prep = None
     if args.precision_report and world == 1:
         prep = precision_report(local_rank)
@@ -528,8 +643,20 @@ def main():
     r64, r32, r32c = results[0], results[1], results[2]
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        c = cpu_reference_timing(max_seconds=20.0, max_steps=4, warm=False)
+        c = cpu_reference_timing(max_seconds=20.0, max_steps=4, warmup=0)
         cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if gs is not None:
+        if world == 1 and not args.no_cpu_baseline:
+            gs["cpu_baseline"] = cpu_ground_state_baseline(gs)
+        e128 = gs.pop("energies_rank0")
+        e64 = gs["c64"].pop("energies_rank0")
+        gs["c64"]["max_energy_rel_diff_vs_c128"] = max(abs(a - b) / abs(b) for a, b in zip(e64, e128))
+        for d in (gs, gs["c64"]):
+            d.pop("_steps")
+            d.pop("_grids")
+    energy = ({k: prep[k] for k in ("max_energy_rel_err_c64", "max_energy_rel_err_c64_state", "max_energy_rel_err_c64c",
+                                    "max_norm_drift_c64c", "ms_per_step_median", "max_norm_drift_c64",
+                                    "max_norm_drift_c128")} if prep else precision_check(local_rank))
     line = {"metric": metric, "value": r64["value"], "unit": "site-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r64["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
@@ -537,11 +664,7 @@ def main():
             "fp32": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "dtype": "c64",
                      "speedup_vs_fp64": r32["value"] / r64["value"], "clocks": r32["clocks"],
                      "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2), "c64"),
-                     "energy_error": ({k: prep[k] for k in ("max_energy_rel_err_c64", "max_energy_rel_err_c64_state",
-                                                            "max_energy_rel_err_c64c", "max_norm_drift_c64c",
-                                                            "ms_per_step_median", "max_norm_drift_c64",
-                                                            "max_norm_drift_c128")} if prep else
-                                      "profiles/precision_quench_256cubed.md"),
+                     "energy_error": energy,
                      "compensated": {"value": r32c["value"], "ms_per_step": r32c["ms_per_step"],
                                      "speedup_vs_fp64": r32c["value"] / r64["value"], "clocks": r32c["clocks"],
                                      "note": "gp5cu_stepper_set_compensation: BF16 correction field, "

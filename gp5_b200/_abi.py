@@ -22,6 +22,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "gp5cu.h")
 GP5_OK, GP5_ERR_ARG, GP5_ERR_CUDA, GP5_ERR_NONFINITE, GP5_ERR_TIMEOUT = 0, 1, 2, 3, 4
 GP5_ERR_UNSUPPORTED, GP5_ERR_STATE, GP5_ERR_NOMEM = 5, 6, 7
 GP5_C128, GP5_C64 = 0, 1
+GP5_GEMM_WAIT_DEFAULT_NS = 2_000_000_000
 GP5_FORWARD, GP5_BACKWARD = -1, 1
 GP5_FUNC_GP, GP5_FUNC_LHY, GP5_FUNC_LHY_UNLOCKED = 0, 1, 2
 GP5_POT_NONE, GP5_POT_HARMONIC, GP5_POT_ARRAY = 0, 1, 2
@@ -65,7 +66,7 @@ class SolveDesc(C.Structure):
 
 class SolveResult(C.Structure):
     _fields_ = [("steps", C.c_int), ("converged", C.c_int), ("residual", C.c_double), ("energy", C.c_double),
-                ("mu", C.c_double), ("norm", C.c_double)]
+                ("mu", C.c_double), ("norm", C.c_double), ("steps_c64", C.c_int)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -127,6 +128,9 @@ def lib():
         "gp5cu_stepper_profile": (i, [vp, vp, i, C.POINTER(d), C.POINTER(i), i, C.POINTER(i)]),
         "gp5cu_norm_noalloc": (i, [vp, i, C.POINTER(C.c_int), i, i, d, vp, C.POINTER(d)]),
         "gp5cu_batch_create": (i, [pp, i, C.POINTER(SolveDesc), i, i]),
+        "gp5cu_batch_create_devices": (i, [pp, i, C.POINTER(SolveDesc), i, i, C.POINTER(C.c_int)]),
+        "gp5cu_batch_assign_devices": (i, [i, C.POINTER(SolveDesc), i, C.POINTER(C.c_int)]),
+        "gp5cu_batch_device": (i, [vp, i]),
         "gp5cu_batch_destroy": (i, [vp]),
         "gp5cu_batch_set_state": (i, [vp, i, vp]),
         "gp5cu_batch_get_state": (i, [vp, i, vp]),
@@ -145,6 +149,7 @@ def lib():
         "gp5cu_mlp_forward": (i, [vp, vp, i, vp]),
         "gp5cu_mlp_gradients": (i, [vp, vp, vp, i, vp, C.POINTER(d)]),
         "gp5cu_mlp_train": (i, [vp, vp, vp, i, i, i, C.c_float, C.c_ulonglong, vp]),
+        "gp5cu_mlp_set_wait_bound": (i, [vp, C.c_ulonglong]),
         "gp5cu_gemm_bf16": (i, [vp, C.c_longlong, C.c_longlong, vp, C.c_longlong, C.c_longlong, vp,
                                 C.c_longlong, i, i, i, vp]),
     }
@@ -426,21 +431,42 @@ class Stepper:
             pass
 
 
+def solve_descs(solves):
+    arr = (SolveDesc * len(solves))()
+    for k, sd in enumerate(solves):
+        arr[k] = SolveDesc(int(sd["n"]), float(sd["L"]), float(sd["N"]), float(sd.get("c3", -3.0)),
+                           float(sd.get("c4", 2.5)), float(sd.get("omega", 0.0)), float(sd["dt"]))
+    return arr
+
+
+def assign_devices(solves, ndevices: int):
+    """Positions in [0, ndevices) of the device each solve runs on (gp5cu_batch_assign_devices);
+    host-only, no GPU needed."""
+    out = (C.c_int * len(solves))()
+    check(lib().gp5cu_batch_assign_devices(len(solves), solve_descs(solves), int(ndevices), out))
+    return list(out)
+
+
 class Batch:
     """Independent LHY droplet ground-state solves advanced together (gp5cu_batch_*).
 
     solves: list of dicts with n, L, N, c3, c4, omega, dt.
     """
 
-    def __init__(self, solves, precision: int = GP5_C128, device: int = 0):
-        arr = (SolveDesc * len(solves))()
-        for k, sd in enumerate(solves):
-            arr[k] = SolveDesc(int(sd["n"]), float(sd["L"]), float(sd["N"]), float(sd.get("c3", -3.0)),
-                               float(sd.get("c4", 2.5)), float(sd.get("omega", 0.0)), float(sd["dt"]))
+    def __init__(self, solves, precision: int = GP5_C128, device: int = 0, devices: Optional[Sequence[int]] = None):
+        arr = solve_descs(solves)
         self.solves = [dict(sd) for sd in solves]
         h = C.c_void_p()
-        check(lib().gp5cu_batch_create(C.byref(h), len(solves), arr, precision, device))
+        if devices is None:
+            check(lib().gp5cu_batch_create(C.byref(h), len(solves), arr, precision, device))
+        else:
+            devs = (C.c_int * len(devices))(*devices)
+            check(lib().gp5cu_batch_create_devices(C.byref(h), len(solves), arr, precision, len(devices), devs))
         self.h = h
+
+    def device(self, k: int) -> int:
+        """Device ordinal that runs solve k."""
+        return int(lib().gp5cu_batch_device(self.h, k))
 
     def set_state(self, k: int, psi: np.ndarray) -> None:
         a = np.asfortranarray(np.asarray(psi, dtype=np.complex128).reshape((self.solves[k]["n"],) * 3, order="F"))
@@ -525,6 +551,10 @@ class Mlp:
         check(lib().gp5cu_mlp_train(self.h, C.c_void_p(_ptr(x)), C.c_void_p(_ptr(t)), x.shape[0], int(epochs),
                                     int(batch), float(lr), int(seed), C.c_void_p(_ptr(hist))))
         return hist
+
+    def set_wait_bound(self, ns: int) -> None:
+        """Bound of the GEMMs' per-chunk MMA wait (gp5cu_mlp_set_wait_bound)."""
+        check(lib().gp5cu_mlp_set_wait_bound(self.h, int(ns)))
 
     def close(self):
         if getattr(self, "h", None):

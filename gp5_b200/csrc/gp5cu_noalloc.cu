@@ -12,11 +12,16 @@
 // exits.  Host code may not pass the array's name to a kernel (on the host the name is only
 // a stand-in, not a device address), so the first call on each device looks up the device
 // address with cudaGetSymbolAddress, with that device current, and caches it.  Because of
-// that look-up, make the first call on a device before any stream capture.
+// that look-up, make the first call on a device before any stream capture.  The cache is
+// keyed by the device and the unique id of its current CUDA context: after a
+// cudaDeviceReset (or any other re-creation of the context) the first call looks the
+// address up again instead of using one from the destroyed context.
 //
 // Sharing: every call uses the same array and leaves the last call's contents in it; the
 // ticket is cleared at the start of each call.  Calls whose kernels overlap on the GPU (for
-// example on two streams at once) race on the array and must not be issued.
+// example on two streams at once) race on the array and must not be issued.  Each call reads
+// the result back and synchronises `stream` before it returns.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -106,11 +111,39 @@ __global__ void __launch_bounds__(kThreadsNA) k_norm_noalloc(const cpx<Real> *__
 }
 
 std::mutex g_mu;
+// per device: the scratch address and the id of the context it was looked up in
 void *g_scratch_addr[64] = {nullptr};
+unsigned long long g_scratch_ctx[64] = {0};
 
 int fail_na(int status, const std::string &msg) {
     gp5::set_last_error(msg);
     return status;
+}
+
+// Unique id of the calling thread's current CUDA context (0 if none can be had).  The driver
+// functions come through cudaGetDriverEntryPoint, so the library needs no link to libcuda.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f1);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f2);
+        looked_up = true;
+    }
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS)
+        return id;
+    return 0;
 }
 
 }  // namespace
@@ -118,19 +151,23 @@ int fail_na(int status, const std::string &msg) {
 extern "C" int gp5cu_norm_noalloc(const void *dfield, int precision, const int shape[3], int ncomp, int comp,
                                   double dV, void *stream, double *out) {
     if (!dfield || !shape || !out) return fail_na(GP5_ERR_ARG, "NULL argument");
-    if (((uintptr_t)dfield & 15u) != 0) return fail_na(GP5_ERR_ARG, "dfield is not 16-byte aligned");
     if (precision != GP5_C128 && precision != GP5_C64)
         return fail_na(GP5_ERR_ARG, "precision must be GP5_C128 or GP5_C64");
+    // one complex element: 16 bytes (double2) or 8 bytes (float2)
+    const uintptr_t align = precision == GP5_C128 ? 16u : 8u;
+    if (((uintptr_t)dfield & (align - 1)) != 0)
+        return fail_na(GP5_ERR_ARG, precision == GP5_C128 ? "dfield is not 16-byte aligned"
+                                                          : "dfield is not 8-byte aligned");
     if (ncomp < 1 || comp < 0 || comp >= ncomp) return fail_na(GP5_ERR_ARG, "component out of range");
     long long nsites = 1;
     for (int d = 0; d < 3; d++) {
         if (shape[d] < 1) return fail_na(GP5_ERR_ARG, "shape entries must be positive");
+        // the limit is checked before each product, so the count never overflows
+        if ((long long)shape[d] > kMaxSites / nsites)
+            return fail_na(GP5_ERR_ARG, "gp5cu_norm_noalloc: the field exceeds the static scratch limit of " +
+                                            std::to_string(kMaxSites) + " sites (GP5_NOALLOC_MAX_SITES); use gp5cu_norm");
         nsites *= shape[d];
     }
-    if (nsites > kMaxSites)
-        return fail_na(GP5_ERR_ARG, "gp5cu_norm_noalloc: " + std::to_string(nsites) +
-                                        " sites exceed the static scratch limit of " + std::to_string(kMaxSites) +
-                                        " (GP5_NOALLOC_MAX_SITES); use gp5cu_norm");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail_na(GP5_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
@@ -138,13 +175,15 @@ extern "C" int gp5cu_norm_noalloc(const void *dfield, int precision, const int s
     void *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_addr[dev]) {
-            // set-up, once per device, with that device current
+        const unsigned long long ctx = current_context_id();
+        if (!g_scratch_addr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
+            // set-up, once per device (and again for a new context), with that device current
             void *ptr = nullptr;
             e = cudaGetSymbolAddress(&ptr, g_norm_scratch);
             if (e != cudaSuccess || !ptr)
                 return fail_na(GP5_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             g_scratch_addr[dev] = ptr;
+            g_scratch_ctx[dev] = current_context_id();
         }
         scratch = g_scratch_addr[dev];
     }

@@ -34,7 +34,8 @@ using bf16 = __nv_bfloat16;
 constexpr int kGemmThreads = 128;  // 4 warps: warp w owns TMEM lanes 32w..32w+31 (rows)
 constexpr int kTileM = 128;
 constexpr int kTileK = 64;
-constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every mbarrier wait (2 s)
+// default bound of the per-chunk MMA wait, and the fixed bound of the drain wait after a timeout
+constexpr unsigned long long kWaitNs = GP5_GEMM_WAIT_DEFAULT_NS;  // 2 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -48,12 +49,23 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 
-// Waits for the phase with the given parity; false once timeout_ns has passed.
+// Waits for the phase with the given parity; false once timeout_ns has passed.  The first
+// probe does not block (test_wait), so a bound of 0 returns false whenever the phase is not
+// complete at the call; later probes use try_wait.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned long long timeout_ns) {
     const uint32_t a = smem_u32(bar);
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
     const unsigned long long t0 = globaltimer_ns();
     while (true) {
-        uint32_t ok;
+        if (globaltimer_ns() - t0 >= timeout_ns) return false;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -62,7 +74,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsign
             : "r"(a), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (globaltimer_ns() - t0 > timeout_ns) return false;
     }
 }
 
@@ -96,6 +107,9 @@ struct GemmArgs {
     float beta;
     int gelu;
     unsigned *err;
+    // bound of each K chunk's MMA wait; on timeout the CTA drains its MMAs (fixed 2 s bound),
+    // sets *err and returns
+    unsigned long long wait_ns = kWaitNs;
 };
 
 __device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
@@ -175,7 +189,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) k_gemm_tc(const GemmArgs a) {
                          : "memory");
         }
         // every thread waits for the MMAs before the tiles are overwritten or TMEM is read
-        if (!mbar_wait(&bar, phase, kWaitNs)) failed = 1;
+        if (!mbar_wait(&bar, phase, a.wait_ns)) failed = 1;
         phase ^= 1u;
         __syncthreads();
     }
@@ -307,6 +321,7 @@ struct gp5cu_mlp {
     bf16 *p16 = nullptr;                                                 // BF16 copies
     unsigned *err = nullptr;
     double *loss = nullptr;
+    unsigned long long wait_ns = GP5_GEMM_WAIT_DEFAULT_NS;  // per-chunk MMA wait bound of its GEMMs
     int cap = 0;  // batch capacity of the buffers below
     bf16 *x16 = nullptr, *act16[L] = {}, *d16 = nullptr;
     float *pre[L] = {}, *act32 = nullptr, *y32 = nullptr, *t32 = nullptr, *d32a = nullptr, *d32b = nullptr;
@@ -372,6 +387,7 @@ void forward(gp5cu_mlp *n, int B) {
         a.bias = n->p32 + n->boff[l];
         a.ld = n->fan_out[l];
         a.err = n->err;
+        a.wait_ns = n->wait_ns;
         if (l < gp5cu_mlp::L - 1) {
             a.pre32 = n->pre[l];
             a.gelu = 1;
@@ -408,6 +424,7 @@ void backward(gp5cu_mlp *n, int B) {
         gw.out32 = n->g32 + n->woff[l];
         gw.ld = fin;
         gw.err = n->err;
+        gw.wait_ns = n->wait_ns;
         launch_gemm(gw, n->stream);
         k_bias_grad<<<(fout + 255) / 256, 256, 0, n->stream>>>(n->d32a, n->g32 + n->boff[l], B, fout);
         ck(cudaGetLastError(), "k_bias_grad");
@@ -426,6 +443,7 @@ void backward(gp5cu_mlp *n, int B) {
         gx.out32 = n->d32b;
         gx.ld = fin;
         gx.err = n->err;
+        gx.wait_ns = n->wait_ns;
         launch_gemm(gx, n->stream);
         // through the GELU of layer l-1
         k_gelu_back<<<256, 256, 0, n->stream>>>(n->d32b, n->pre[l - 1], n->d16, n->d32a, (long long)B * fin);
@@ -434,11 +452,22 @@ void backward(gp5cu_mlp *n, int B) {
     }
 }
 
+// A bounded device wait ran out: reported as GP5_ERR_TIMEOUT.
+struct WaitTimeout {
+    std::string msg;
+};
+
+// Reads the GEMM error flag of the net's stream; a set flag is cleared (so the next call on
+// the handle starts clean) and reported as a timeout.
 void check_err(gp5cu_mlp *n) {
     unsigned e = 0;
     ck(cudaMemcpyAsync(&e, n->err, sizeof(unsigned), cudaMemcpyDeviceToHost, n->stream), "read err");
     ck(cudaStreamSynchronize(n->stream), "sync");
-    if (e) throw std::string("tensor-core GEMM: a bounded mbarrier wait ran out");
+    if (e) {
+        ck(cudaMemsetAsync(n->err, 0, sizeof(unsigned), n->stream), "clear err");
+        ck(cudaStreamSynchronize(n->stream), "sync");
+        throw WaitTimeout{"tensor-core GEMM: a bounded mbarrier wait ran out"};
+    }
 }
 
 void upload_xt(gp5cu_mlp *n, const float *x, const float *t, int B) {
@@ -461,6 +490,9 @@ int fail_m(int st, const std::string &m) {
 
 #define MLP_TRY try {
 #define MLP_CATCH                                   \
+    }                                               \
+    catch (const WaitTimeout &e) {                  \
+        return fail_m(GP5_ERR_TIMEOUT, e.msg);      \
     }                                               \
     catch (const std::string &e) {                  \
         return fail_m(GP5_ERR_CUDA, e);             \
@@ -532,6 +564,12 @@ int gp5cu_mlp_destroy(gp5cu_mlp *n) {
 }
 
 long long gp5cu_mlp_num_params(const gp5cu_mlp *n) { return n ? n->nparam : 0; }
+
+int gp5cu_mlp_set_wait_bound(gp5cu_mlp *n, unsigned long long ns) {
+    if (!n) return fail_m(GP5_ERR_ARG, "NULL argument");
+    n->wait_ns = ns;
+    return GP5_OK;
+}
 
 int gp5cu_mlp_get_params(gp5cu_mlp *n, float *host) {
     if (!n || !host) return fail_m(GP5_ERR_ARG, "NULL argument");
@@ -656,7 +694,7 @@ int gp5cu_gemm_bf16(const void *A, long long sam, long long sak, const void *B, 
         throw;
     }
     cudaFree(err);
-    if (e) throw std::string("tensor-core GEMM: a bounded mbarrier wait ran out");
+    if (e) throw WaitTimeout{"tensor-core GEMM: a bounded mbarrier wait ran out"};
     MLP_CATCH
 }
 

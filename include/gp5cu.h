@@ -190,8 +190,16 @@ int gp5cu_stepper_profile(gp5cu_stepper *st, void *dfield, int nrep, double *ms,
  * protocol is python/test/regressionTests/LHY_imaginary.py).  Many LHY droplet solves, each
  * on its own cubic grid, box, atom number, coefficients and time step, advance together:
  * solves of the same grid size share every kernel launch (one launch per pass covers all of
- * them), the steps between convergence checks replay from one CUDA graph, and solves that
- * reach the residual tolerance stop (their tiles return at once). */
+ * them), the steps between convergence checks replay from CUDA graphs, and solves that reach
+ * the residual tolerance stop: at the next check the solves still running are packed into
+ * the first slots of their group and the launches shrink to them, so a long tail of slow
+ * solves does not pay for the finished ones.
+ * precision GP5_C64: every solve first runs with complex64 transforms and state (FP64
+ * reductions) until its residual is at most GP5_BATCH_SWITCH_RESIDUAL or stops falling near
+ * the complex64 floor (rounding of the FP32 state, amplified by the kinetic operator, keeps
+ * the residual above about 1e-6); the state is then converted to complex128 and the solve
+ * continues in complex128 to `tol`. */
+#define GP5_BATCH_SWITCH_RESIDUAL 1e-5
 typedef struct gp5cu_batch gp5cu_batch;
 
 typedef struct gp5cu_solve_desc {
@@ -208,10 +216,24 @@ typedef struct gp5cu_solve_result {
     int converged;    /* residual <= tol */
     double residual;  /* ||H psi - mu psi|| / ||psi|| at the last check */
     double energy, mu, norm;
+    int steps_c64;    /* of `steps`, those taken in complex64 (GP5_C64 batches; 0 otherwise) */
 } gp5cu_solve_result;
 
 int gp5cu_batch_create(gp5cu_batch **out, int nsolves, const gp5cu_solve_desc *solves, int precision,
                        int device);
+/* The same over several GPUs of one process: the solves are split by index over `devices`
+ * (gp5cu_batch_assign_devices) and every device runs its own groups; the solves are
+ * independent, so nothing moves between devices (no collective, no peer access).  One host
+ * thread drives all devices: their launches are asynchronous, so the devices work at once
+ * and the host waits for each at the convergence checks. */
+int gp5cu_batch_create_devices(gp5cu_batch **out, int nsolves, const gp5cu_solve_desc *solves, int precision,
+                               int ndevices, const int *devices);
+/* The split used by gp5cu_batch_create_devices, computed on the host only: solves in order of
+ * decreasing grid sites (ties by index), each to the device position with the fewest sites so
+ * far (ties to the lower position).  device_index[i] receives a position in [0, ndevices). */
+int gp5cu_batch_assign_devices(int nsolves, const gp5cu_solve_desc *solves, int ndevices, int *device_index);
+/* Device ordinal of one solve (-1 for a bad argument). */
+int gp5cu_batch_device(const gp5cu_batch *b, int solve);
 int gp5cu_batch_destroy(gp5cu_batch *b);
 /* Initial / current state of one solve, complex128 host data of n^3 elements. */
 int gp5cu_batch_set_state(gp5cu_batch *b, int solve, const double *host_c128);
@@ -264,6 +286,13 @@ int gp5cu_mlp_train(gp5cu_mlp *net, const float *x, const float *t, int count, i
  * BF16 device operands, FP32 device result, on `stream` (cudaStream_t or NULL; synchronised) */
 int gp5cu_gemm_bf16(const void *A, long long sam, long long sak, const void *B, long long sbn, long long sbk,
                     float *C, long long ldc, int M, int N, int K, void *stream);
+/* Bound of the tensor-core GEMMs' device-side wait for each K chunk's MMAs, for the net's
+ * later calls (default GP5_GEMM_WAIT_DEFAULT_NS = 2 s).  When a wait runs out, the CTA stops,
+ * waits (with the fixed 2 s bound) for the MMAs it issued, frees its tensor memory and flags
+ * the error; the call then returns GP5_ERR_TIMEOUT and the net stays usable.  A bound of 0
+ * fails every wait whose MMAs have not completed at the first probe (used to test the path). */
+#define GP5_GEMM_WAIT_DEFAULT_NS 2000000000ULL
+int gp5cu_mlp_set_wait_bound(gp5cu_mlp *net, unsigned long long ns);
 
 /* ---- tile-shape autotuner ----------------------------------------------------------------
  * No reference counterpart (FFTW plans its own transforms).  The strided y/z passes of the
@@ -288,10 +317,12 @@ int gp5cu_plan_set_tiles(gp5cu_plan *plan, const int threads[5]);
  * array of 33,024 bytes that every GPU loading the library keeps until the process exits.
  * Limit: at most GP5_NOALLOC_MAX_SITES sites (256^3); larger fields return GP5_ERR_ARG.
  * dfield: device field (shape[0]*shape[1]*shape[2] sites, ncomp components, `precision`) on
- * the current device; stream: cudaStream_t or NULL; *out receives the norm (host), after
- * the stream is synchronised.  The first call on a device looks up the scratch address
- * (cudaGetSymbolAddress): make it before any stream capture.  Calls share the scratch, so
- * calls that overlap on the GPU race. */
+ * the current device, 16-byte aligned for GP5_C128 and 8-byte aligned for GP5_C64; stream:
+ * cudaStream_t or NULL; *out receives the norm (host): the call reads it back and
+ * synchronises `stream` before it returns.  The first call on a device (and the first after
+ * its CUDA context is re-created) looks up the scratch address (cudaGetSymbolAddress): make
+ * it before any stream capture.  Calls share the scratch, so calls that overlap on the GPU
+ * race. */
 #define GP5_NOALLOC_MAX_SITES 16777216LL
 int gp5cu_norm_noalloc(const void *dfield, int precision, const int shape[3], int ncomp, int comp,
                        double dV, void *stream, double *out);

@@ -107,3 +107,26 @@ def test_training_reduces_loss():
     assert hist[-1] < 0.05 * hist[0]
     y = net.forward(x).astype(np.float64)
     assert np.mean((y - t) ** 2) < 0.05 * np.mean(t ** 2)
+
+
+def test_gemm_wait_timeout_returns_timeout_status_and_net_stays_usable():
+    """A per-chunk MMA wait bound of 0 makes the first wait run out (the MMAs cannot have
+    finished at the first, non-blocking probe); the CTA drains its MMAs with the fixed 2 s
+    bound, frees its tensor memory and flags the error.  The call returns GP5_ERR_TIMEOUT (not
+    GP5_ERR_CUDA), and the next forward on the same handle, with the default bound, matches
+    the oracle."""
+    from gp5_b200 import _abi
+    p = mo.init_params(21)
+    net = _net_with(p)
+    rng = np.random.default_rng(6)
+    x = rng.standard_normal((256, 3)).astype(np.float32)
+    net.set_wait_bound(0)
+    with pytest.raises(_abi.Gp5Error) as ei:
+        net.forward(x)
+    assert ei.value.status == _abi.GP5_ERR_TIMEOUT
+    assert b"bounded mbarrier wait ran out" in _abi.lib().gp5cu_last_error()
+    net.set_wait_bound(_abi.GP5_GEMM_WAIT_DEFAULT_NS)
+    for _ in range(2):
+        y = net.forward(x).astype(np.float64)
+        yq, _ = mo.forward(p, x, quantize=True)
+        assert np.max(np.abs(y - yq)) <= 2e-3 * np.max(np.abs(yq))
