@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "libgp5cu.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "gp5cu.h")
 
 GP5_OK, GP5_ERR_ARG, GP5_ERR_CUDA, GP5_ERR_NONFINITE, GP5_ERR_TIMEOUT = 0, 1, 2, 3, 4
-GP5_ERR_UNSUPPORTED, GP5_ERR_STATE, GP5_ERR_NOMEM = 5, 6, 7
+GP5_ERR_UNSUPPORTED, GP5_ERR_STATE, GP5_ERR_NOMEM, GP5_ERR_IO = 5, 6, 7, 8
 GP5_C128, GP5_C64 = 0, 1
 GP5_GEMM_WAIT_DEFAULT_NS = 2_000_000_000
 GP5_FORWARD, GP5_BACKWARD = -1, 1
@@ -127,6 +127,12 @@ def lib():
         "gp5cu_stepper_launches_per_step": (i, [vp]),
         "gp5cu_stepper_profile": (i, [vp, vp, i, C.POINTER(d), C.POINTER(i), i, C.POINTER(i)]),
         "gp5cu_norm_noalloc": (i, [vp, i, C.POINTER(C.c_int), i, i, d, vp, C.POINTER(d)]),
+        "gp5cu_h5_save_field": (i, [C.c_char_p, vp, C.POINTER(C.c_int), i]),
+        "gp5cu_h5_field_shape": (i, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "gp5cu_h5_load_field": (i, [C.c_char_p, vp, C.POINTER(C.c_int), i]),
+        "gp5cu_h5_dataset_info": (i, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                      C.POINTER(C.c_int)]),
+        "gp5cu_h5_read_dataset": (i, [C.c_char_p, C.c_char_p, vp, C.c_longlong]),
         "gp5cu_batch_create": (i, [pp, i, C.POINTER(SolveDesc), i, i]),
         "gp5cu_batch_create_devices": (i, [pp, i, C.POINTER(SolveDesc), i, i, C.POINTER(C.c_int)]),
         "gp5cu_batch_assign_devices": (i, [i, C.POINTER(SolveDesc), i, C.POINTER(C.c_int)]),
@@ -429,6 +435,43 @@ class Stepper:
             self.close()
         except Exception:
             pass
+
+
+def h5_save_field(path: str, psi: np.ndarray) -> None:
+    """Writes a (nx, ny, nz[, ncomp]) complex field to an HDF5 file in the reference's layout
+    (gp5cu_h5_save_field)."""
+    a = np.asarray(psi)
+    if a.ndim == 3:
+        a = a[..., None]
+    a = np.asfortranarray(a.astype(np.complex128, copy=False))
+    check(lib().gp5cu_h5_save_field(os.fsencode(path), C.c_void_p(_ptr(a)), (C.c_int * 3)(*a.shape[:3]),
+                                    a.shape[3]))
+
+
+def h5_field_shape(path: str):
+    """((nx, ny, nz), ncomp) of the "field" dataset of an HDF5 file."""
+    s, nc = (C.c_int * 3)(), C.c_int()
+    check(lib().gp5cu_h5_field_shape(os.fsencode(path), s, C.byref(nc)))
+    return tuple(s), nc.value
+
+
+def h5_load_field(path: str) -> np.ndarray:
+    """The "field" dataset of an HDF5 file as a (nx, ny, nz, ncomp) complex128 array."""
+    shape, nc = h5_field_shape(path)
+    out = np.empty(shape + (nc,), dtype=np.complex128, order="F")
+    check(lib().gp5cu_h5_load_field(os.fsencode(path), C.c_void_p(_ptr(out)), (C.c_int * 3)(*shape), nc))
+    return out
+
+
+def h5_read_dataset(path: str, name: str) -> np.ndarray:
+    """Any float64 dataset (real or complex) of the root group, with its HDF5 dims."""
+    rank, dims, cplx = C.c_int(), (C.c_longlong * 8)(), C.c_int()
+    check(lib().gp5cu_h5_dataset_info(os.fsencode(path), name.encode(), C.byref(rank), dims, C.byref(cplx)))
+    shape = tuple(dims[k] for k in range(rank.value))
+    n = int(np.prod(shape, dtype=np.int64)) * (2 if cplx.value else 1)
+    out = np.empty(n, dtype=np.float64)
+    check(lib().gp5cu_h5_read_dataset(os.fsencode(path), name.encode(), C.c_void_p(_ptr(out)), n))
+    return out.view(np.complex128).reshape(shape) if cplx.value else out.reshape(shape)
 
 
 def solve_descs(solves):

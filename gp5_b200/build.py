@@ -25,7 +25,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                   "-I" + os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["gp5cu_f64.cu", "gp5cu_f32.cu", "gp5cu_host.cu", "gp5cu_batch.cu", "gp5cu_noalloc.cu", "mlp.cu", "gp5cu_cluster.cu"]
+CU_SOURCES = ["gp5cu_f64.cu", "gp5cu_f32.cu", "gp5cu_host.cu", "gp5cu_batch.cu", "gp5cu_noalloc.cu", "mlp.cu",
+              "gp5cu_cluster.cu", "gp5cu_h5.cpp"]
 HEADERS = ["common.cuh", "fft_line.cuh", "passes.cuh", "ops.cuh", "launch_impl.cuh", "plan.hpp"]
 
 
@@ -54,7 +55,7 @@ def build_lib(verbose: bool = False, ptxas_info: bool = False) -> str:
     objs, jobs = [], []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if _newer(o, [s] + hdrs) or ptxas_info:
             extra = ["-Xptxas", "-v"] if ptxas_info else []

@@ -413,6 +413,7 @@ const char *gp5cu_status_string(int status) {
         case GP5_ERR_UNSUPPORTED: return "unsupported";
         case GP5_ERR_STATE: return "invalid state";
         case GP5_ERR_NOMEM: return "out of device memory";
+        case GP5_ERR_IO: return "file error";
         default: return "unknown status";
     }
 }

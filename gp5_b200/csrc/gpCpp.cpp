@@ -109,6 +109,23 @@ public:
         check(gp5cu_upload_c128(_plan->p, _d, reinterpret_cast<const double *>(arr.data())));
     }
 
+    // field::save / field::load (src/gpCpp.cpp:105-118): the reference's HDF5 layout
+    // (src/io.cpp:56-256), dataset "field" [nComp][Nz][Ny][Nx] of complex (array of 2 doubles)
+    void save(const std::string &filename) const {
+        const auto s = _geo.getShape();
+        std::vector<std::complex<double>> h((size_t)s[0] * s[1] * s[2] * _nc);
+        check(gp5cu_download_c128(_plan->p, _d, reinterpret_cast<double *>(h.data())));
+        const int shape[3] = {s[0], s[1], s[2]};
+        check(gp5cu_h5_save_field(filename.c_str(), reinterpret_cast<const double *>(h.data()), shape, _nc));
+    }
+    void load(const std::string &filename) {
+        const auto s = _geo.getShape();
+        std::vector<std::complex<double>> h((size_t)s[0] * s[1] * s[2] * _nc);
+        const int shape[3] = {s[0], s[1], s[2]};
+        check(gp5cu_h5_load_field(filename.c_str(), reinterpret_cast<double *>(h.data()), shape, _nc));
+        check(gp5cu_upload_c128(_plan->p, _d, reinterpret_cast<const double *>(h.data())));
+    }
+
     double getNorm(int c) const {
         double n = 0;
         check(gp5cu_norm(_plan->p, _d, c, &n));
@@ -315,6 +332,8 @@ PYBIND11_MODULE(gpCpp, m) {
         .def("getOffset", &field::getOffset)
         .def("getNorm", &field::getNorm)
         .def("normalize", &field::normalize)
+        .def("save", &field::save)
+        .def("load", &field::load)
         .def("maxDensity", &field::maxDensity);
     py::class_<model>(m, "model")
         .def("apply", &model::apply)

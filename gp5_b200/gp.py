@@ -6,9 +6,10 @@ Differences from the reference:
   * ``field.array`` returns a host copy of the device state (assign to it to upload);
   * ``field(..., precision="c64")`` selects complex64 bulk arithmetic;
   * ``GP`` (harmonic GP model) and ``model.observables`` (E, mu, residual) are extensions;
-  * ``save``/``load`` write the state in the reference's HDF5 layout when h5py is present
-    (dataset "field", element double[2], dims [nComp][Nz][Ny][Nx], src/io.cpp:41-135),
-    otherwise the same bytes as a .npy file (complex128, the HDF5 payload order).
+  * ``save``/``load`` of .hdf5/.h5 files use the reference's HDF5 layout (dataset "field",
+    element double[2], dims [nComp][Nz][Ny][Nx], src/io.cpp:41-135) through gpCpp.field.save
+    and gpCpp.field.load, which read and write the format without libhdf5 or h5py; a .npy file
+    name stores the same payload as a numpy array.
 """
 from __future__ import annotations
 
@@ -119,14 +120,10 @@ class field:
             raise RuntimeError("Unknown format {}".format(format))
 
     def saveHDF5(self, filename):
-        try:
-            import h5py
-        except ImportError as e:
-            raise RuntimeError("HDF5 output needs h5py; use a .npy file name") from e
-        psi = self.array  # (nx, ny, nz, nc) -> dims [nc][nz][ny][nx], element double[2]
-        data = np.ascontiguousarray(np.transpose(psi, (3, 2, 1, 0)))
-        with h5py.File(filename, "w") as f:
-            f.create_dataset("field", data=data.view(np.float64).reshape(data.shape + (2,)))
+        """gp.field.saveHDF5 (python/gp/gp.py:127-131) through gpCpp.field.save: the
+        reference's HDF5 layout (src/io.cpp:56-152), written by the library itself."""
+        Path(os.path.dirname(filename) or ".").mkdir(parents=True, exist_ok=True)
+        self._fieldCpp.save(filename)
 
     def saveNetCDF(self, filename):
         from netCDF4 import Dataset
@@ -147,13 +144,10 @@ class field:
         root.close()
 
     def load(self, filename):
+        """gp.field.load (python/gp/gp.py:161-162): HDF5 files in the reference's layout
+        (src/io.cpp:154-256) through gpCpp.field.load; .npy files hold the same payload."""
         if re.match(r".*\.(hdf5|h5)$", filename):
-            import h5py
-
-            with h5py.File(filename, "r") as f:
-                d = np.asarray(f["field"])
-            c = d[..., 0] + 1j * d[..., 1]
-            self.array = np.transpose(c, (3, 2, 1, 0))
+            self._fieldCpp.load(filename)
         else:
             self.array = np.load(filename)
 

@@ -17,10 +17,11 @@ src/constraint.cpp:19-37):
 Loop (src/main.cpp:176-205): while t <= maxTime: save the state to <folder>/out_<k>; advance
 nIterations steps (t += timeStep per step); k += 1.
 
-Files: the reference reads and writes HDF5 (src/io.cpp).  HDF5 needs libhdf5 (or h5py), which
-this environment does not have; fields, potentials and phases are read from and written to
-.npy files holding the same payload, a (nx, ny, nz, ncomp) array in x-fastest order.  A .hdf5
-/ .h5 path is read or written through h5py when it is importable.
+Files: fields, potentials and phases are HDF5 files in the reference's layout (src/io.cpp:
+dataset "field", complex elements, dims [nComp][Nz][Ny][Nx]), read and written by the
+library's own HDF5 code (gp5cu_h5_*); the states are saved as <folder>/out_<k>.hdf5 like the
+reference's executable (src/main.cpp:193).  A .npy path holds the same payload as a
+(nx, ny, nz, ncomp) numpy array.
 """
 from __future__ import annotations
 
@@ -116,29 +117,25 @@ def build_spec(cfg: dict) -> dict:
 
 
 def read_array(path: str, base: str = "") -> np.ndarray:
+    """A field, potential or phase file (gp::load, src/io.cpp:154-256) as a (nx, ny, nz, ncomp)
+    complex array; .npy files hold the same payload."""
     p = path if os.path.isabs(path) or not base else os.path.join(base, path)
     if p.endswith((".hdf5", ".h5")):
         try:
-            import h5py
-        except ImportError as e:
-            raise ConfigError(f"{p}: reading HDF5 needs h5py, which is not installed; give a .npy file") from e
-        with h5py.File(p, "r") as f:
-            d = np.asarray(f["field"])
-        # dataset [nComp][Nz][Ny][Nx] of double[2] (src/io.cpp:41-45,77-85)
-        a = d[..., 0] + 1j * d[..., 1] if d.ndim == 5 else d
-        return np.asfortranarray(np.transpose(a, (3, 2, 1, 0)))
+            return _abi.h5_load_field(p)
+        except _abi.Gp5Error as e:
+            raise ConfigError(f"{p}: {e}") from e
     return np.load(p)
 
 
 def write_array(path: str, a: np.ndarray) -> str:
-    if path.endswith((".hdf5", ".h5")):
-        import h5py
-        d = np.transpose(np.asarray(a), (3, 2, 1, 0))
-        with h5py.File(path, "w") as f:
-            f.create_dataset("field", data=np.stack([d.real, d.imag], axis=-1))
+    """Saves a field (gp::save, src/io.cpp:56-152): HDF5 unless the path ends in .npy; a path
+    without an extension gets .hdf5 (out_<k>.hdf5, src/main.cpp:193).  Returns the file name."""
+    if path.endswith(".npy"):
+        np.save(path, np.asfortranarray(a))
         return path
-    p = path if path.endswith(".npy") else path + ".npy"
-    np.save(p, np.asfortranarray(a))
+    p = path if path.endswith((".hdf5", ".h5")) else path + ".hdf5"
+    _abi.h5_save_field(p, np.asarray(a))
     return p
 
 

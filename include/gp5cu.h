@@ -36,6 +36,7 @@ extern "C" {
 #define GP5_ERR_UNSUPPORTED 5 /* size/radix/feature not supported */
 #define GP5_ERR_STATE 6       /* object used in the wrong state */
 #define GP5_ERR_NOMEM 7       /* device allocation failed */
+#define GP5_ERR_IO 8          /* a file could not be read or written, or is malformed */
 
 /* ---- enums ---- */
 #define GP5_C128 0 /* complex128 bulk arithmetic */
@@ -308,6 +309,27 @@ int gp5cu_mlp_set_wait_bound(gp5cu_mlp *net, unsigned long long ns);
 int gp5cu_plan_autotune(gp5cu_plan *plan);
 int gp5cu_plan_get_tiles(const gp5cu_plan *plan, int threads[5]);
 int gp5cu_plan_set_tiles(gp5cu_plan *plan, const int threads[5]);
+
+/* ---- HDF5 field files ----------------------------------------------------------------------
+ * The reference's on-disk format, read and written without libhdf5 (host only, no GPU):
+ * gp::save / gp::load (src/io.cpp:56-152, 154-256), bound as field.save / field.load
+ * (src/gpCpp.cpp:105-118, 343-344).  One dataset "field" in the root group, element
+ * H5Tarray(double, [2]) (src/io.cpp:45), dims [nComp][Nz][Ny][Nx], contiguous; its raw data is
+ * the field's memory order (x fastest, components slowest), so host_c128 is the same buffer
+ * gp5cu_upload / gp5cu_download use.  save writes superblock 0, version-1 object headers and a
+ * symbol-table root group; load also reads superblocks 0-3 (with a user block), version-2
+ * object headers, link-message groups and complex elements stored as a compound of two
+ * doubles, from contiguous or compact storage.  Errors: GP5_ERR_IO (file), GP5_ERR_ARG (no
+ * "field" dataset, or a shape other than the one requested), GP5_ERR_UNSUPPORTED (chunked,
+ * filtered or dense-link storage). */
+int gp5cu_h5_save_field(const char *path, const double *host_c128, const int shape[3], int ncomp);
+int gp5cu_h5_field_shape(const char *path, int shape[3], int *ncomp);
+int gp5cu_h5_load_field(const char *path, double *host_c128, const int shape[3], int ncomp);
+/* Any float64 dataset of the root group: its rank, dims (slowest first, at most 8) and whether
+ * its element is complex (two doubles); then its values as doubles (count = product of dims,
+ * times 2 when complex). */
+int gp5cu_h5_dataset_info(const char *path, const char *name, int *rank, long long dims[8], int *complex_elems);
+int gp5cu_h5_read_dataset(const char *path, const char *name, double *out, long long count);
 
 /* ---- allocation-free norm ---------------------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc when they need

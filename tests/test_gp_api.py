@@ -157,3 +157,26 @@ def test_gp_model_observables_and_precision():
     st64 = gp.stepper(model, 1e-3)
     st64.advance(psi, 10)
     assert np.max(np.abs(psi32.array - psi.array)) < 1e-5 * np.max(np.abs(psi.array))
+
+
+@pytest.mark.gpu
+def test_field_save_load_hdf5(tmp_path):
+    """gp.field.save / load of .hdf5 files (python/gp/gp.py:101-162 -> gpCpp.field.save / load,
+    src/gpCpp.cpp:105-118) in the reference's layout (src/io.cpp: dataset "field",
+    [nComp][Nz][Ny][Nx] of double[2]), through the library's own HDF5 writer and reader."""
+    from gp5_b200 import _abi, gp
+    geo = gp.geometry((12, 10, 8), left=[-3, -2, -1], right=[3, 2, 1])
+    psi = gp.field(geo, nComponents=2)
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((12, 10, 8, 2)) + 1j * rng.standard_normal((12, 10, 8, 2))
+    psi.array = a
+    p = str(tmp_path / "sub" / "state.hdf5")
+    psi.save(p)
+    assert _abi.h5_field_shape(p) == ((12, 10, 8), 2)
+    assert np.array_equal(_abi.h5_read_dataset(p, "field"), np.transpose(a, (3, 2, 1, 0)))
+    other = gp.field(geo, nComponents=2)
+    other.load(p)
+    assert np.array_equal(other.array, a)
+    wrong = gp.field(gp.geometry((12, 10, 6)), nComponents=2)
+    with pytest.raises(RuntimeError):
+        wrong.load(p)

@@ -73,9 +73,16 @@ def test_potential_sum_and_files(tmp_path):
     ref = (X * X + 0.64 * Y * Y + 1.44 * Z * Z) * 0.5 + 0.5 / (X * X + Y * Y) + extra[..., 0]
     assert np.max(np.abs(V[..., 0] - ref)) < 1e-12
     p = R.write_array(str(tmp_path / "f"), extra.astype(complex))
+    assert p.endswith("f.hdf5")
     back = R.read_array(p)
     assert np.array_equal(back, extra) and back.flags["F_CONTIGUOUS"]
-    with pytest.raises(R.ConfigError, match="h5py"):
+    p = R.write_array(str(tmp_path / "g.npy"), extra.astype(complex))
+    assert np.array_equal(R.read_array(p), extra)
+    # a potential given as an HDF5 file in the reference's layout
+    R.write_array(str(tmp_path / "V.hdf5"), extra.astype(complex))
+    c["functional"]["V"]["V"]["c"]["filename"] = str(tmp_path / "V.hdf5")
+    assert np.max(np.abs(R.potential_array(R.build_spec(c))[..., 0] - ref)) < 1e-12
+    with pytest.raises(R.ConfigError, match="cannot open"):
         R.read_array(str(tmp_path / "x.hdf5"))
 
 
@@ -143,5 +150,5 @@ def test_run_loop_outputs_and_time(tmp_path, monkeypatch, max_time):
     assert len(r["files"]) == k and r["steps"] == 10 * k and r["time"] == t
     assert _FakeStepper.calls == [10] * k
     for j, fpath in enumerate(r["files"]):
-        assert fpath.endswith(f"out_{j}.npy") and os.path.dirname(fpath) == str(tmp_path / "out")
-        assert np.all(np.load(fpath) == 10 * j)  # out_j is saved before block j advances
+        assert fpath.endswith(f"out_{j}.hdf5") and os.path.dirname(fpath) == str(tmp_path / "out")
+        assert np.all(R.read_array(fpath) == 10 * j)  # out_j is saved before block j advances
