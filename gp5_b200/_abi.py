@@ -124,6 +124,7 @@ def lib():
         "gp5cu_stepper_get_time": (i, [vp, C.POINTER(d)]),
         "gp5cu_stepper_set_time": (i, [vp, d]),
         "gp5cu_stepper_advance_host": (i, [vp, vp, vp, i]),
+        "gp5cu_stepper_advance_host_many": (i, [vp, i, C.POINTER(vp), C.POINTER(vp), i]),
         "gp5cu_stepper_launches_per_step": (i, [vp]),
         "gp5cu_stepper_profile": (i, [vp, vp, i, C.POINTER(d), C.POINTER(i), i, C.POINTER(i)]),
         "gp5cu_norm_noalloc": (i, [vp, i, C.POINTER(C.c_int), i, i, d, vp, C.POINTER(d)]),
@@ -405,6 +406,15 @@ class Stepper:
     def advance_host(self, host_in: np.ndarray, host_out: np.ndarray, nsteps: int) -> None:
         check(lib().gp5cu_stepper_advance_host(self.h, C.c_void_p(_ptr(host_in)), C.c_void_p(_ptr(host_out)),
                                                int(nsteps)))
+
+    def advance_host_many(self, host_in, host_out, nsteps: int) -> None:
+        """Independent host states, pipelined (gp5cu_stepper_advance_host_many); host_in and
+        host_out are lists of arrays (or of raw addresses) of one field each."""
+        n = len(host_in)
+        addr = lambda a: a if isinstance(a, int) else _ptr(a)  # noqa: E731
+        ins = (C.c_void_p * n)(*[addr(a) for a in host_in])
+        outs = (C.c_void_p * n)(*[addr(a) for a in host_out])
+        check(lib().gp5cu_stepper_advance_host_many(self.h, n, ins, outs, int(nsteps)))
 
     @property
     def time(self) -> float:

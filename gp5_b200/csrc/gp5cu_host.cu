@@ -352,6 +352,16 @@ gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const do
         {
             const char *pdl = std::getenv("GP5_PDL");
             p->pdl = !(pdl && std::string(pdl) == "0");
+            const char *l2o = std::getenv("GP5_L2ORDER");
+            p->l2_order = l2o && std::string(l2o) == "1";
+            const char *sa = std::getenv("GP5_STREAM_AUX");
+            p->stream_aux = sa && std::string(sa) == "1";
+            const char *yz = std::getenv("GP5_YZ_SLABS");
+            if (yz) {
+                const int v = std::atoi(yz);
+                // slabs must split x evenly into whole tiles (x a power of two >= 32 per slab)
+                if (v >= 1 && shape[0] % v == 0 && (shape[0] / v) % 32 == 0) p->yz_slabs = v;
+            }
         }
         p->nsites = (long long)shape[0] * shape[1] * shape[2];
         p->nsolve = nsolve;
@@ -790,12 +800,22 @@ int gp5cu_stepper_destroy(gp5cu_stepper *st) {
     if (!st) return GP5_OK;
     cudaSetDevice(st->func->plan->dev);
     cudaStreamSynchronize(st->func->plan->stream);
-    if (st->exec) cudaGraphExecDestroy(st->exec);
+    drop_graph(st);
+    if (st->up) cudaStreamSynchronize(st->up);
+    if (st->down) cudaStreamSynchronize(st->down);
+    for (int b = 0; b < 2; b++) {
+        if (st->ev_up[b]) cudaEventDestroy(st->ev_up[b]);
+        if (st->ev_done[b]) cudaEventDestroy(st->ev_done[b]);
+        if (st->ev_down[b]) cudaEventDestroy(st->ev_down[b]);
+    }
+    if (st->up) cudaStreamDestroy(st->up);
+    if (st->down) cudaStreamDestroy(st->down);
     cudaFree(st->Ka);
     cudaFree(st->Kb);
     cudaFree(st->ds);
     cudaFree(st->phase_exp);
     cudaFree(st->dstate);
+    cudaFree(st->dstate2);
     cudaFree(st->comp);
     cudaFree(st->sp);
     delete st;
@@ -807,6 +827,9 @@ void drop_graph(gp5cu_stepper *st) {
     if (st->exec) cudaGraphExecDestroy(st->exec);
     st->exec = nullptr;
     st->graph_field = nullptr;
+    if (st->exec_alt) cudaGraphExecDestroy(st->exec_alt);
+    st->exec_alt = nullptr;
+    st->graph_field_alt = nullptr;
 }
 }  // extern "C++"
 
@@ -896,6 +919,15 @@ extern "C++" {
 void build_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps) {
     gp5cu_plan *p = st->func->plan;
     drop_graph(st);
+    capture_graph(st, field, merged, ksteps);
+}
+
+// Captures into the primary graph slot only (the alternate slot is kept).
+void capture_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps) {
+    gp5cu_plan *p = st->func->plan;
+    if (st->exec) cudaGraphExecDestroy(st->exec);
+    st->exec = nullptr;
+    st->graph_field = nullptr;
     p->dry = true;
     try {
         queue_step(st, field, merged, false);
@@ -925,22 +957,33 @@ void build_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps) {
 }
 }  // extern "C++"
 
-int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
-    GP5_TRY
-    require(st != nullptr, "stepper is NULL");
-    check_field_ptr(field, "field");
-    require(nsteps >= 0, "nsteps must be >= 0");
+// Queues nsteps steps of `field` on the plan stream (no synchronisation).  The two most recent
+// fields keep their captured one-step graphs.
+static void enqueue_advance(gp5cu_stepper *st, void *field, int nsteps) {
     gp5cu_plan *p = st->func->plan;
-    use_device(p);
-    if (nsteps == 0) return GP5_OK;
     const bool merged = merged_path(p);
     if (compensation_active(st) && st->comp_field != field) {
         // the correction belongs to one state: a new state starts from zero
         check_cuda(cudaMemsetAsync(st->comp, 0, p->field_bytes / 2 * (size_t)p->nsolve, p->stream), "memset");
         st->comp_field = field;
     }
-    if (!st->exec || st->graph_field != field || st->graph_merged != merged || st->graph_steps != 1)
-        build_graph(st, field, merged, 1);
+    auto fits = [&](cudaGraphExec_t e, void *f, bool m, int k) { return e && f == field && m == merged && k == 1; };
+    if (!fits(st->exec, st->graph_field, st->graph_merged, st->graph_steps)) {
+        if (fits(st->exec_alt, st->graph_field_alt, st->graph_merged_alt, st->graph_steps_alt)) {
+            std::swap(st->exec, st->exec_alt);
+            std::swap(st->graph_field, st->graph_field_alt);
+            std::swap(st->graph_merged, st->graph_merged_alt);
+            std::swap(st->graph_steps, st->graph_steps_alt);
+        } else {
+            if (st->exec_alt) cudaGraphExecDestroy(st->exec_alt);
+            st->exec_alt = st->exec;
+            st->graph_field_alt = st->graph_field;
+            st->graph_merged_alt = st->graph_merged;
+            st->graph_steps_alt = st->graph_steps;
+            st->exec = nullptr;
+            capture_graph(st, field, merged, 1);
+        }
+    }
     set_scalars(p->stream, st->ds, p->nsolve);
     if (merged) {
         // forward x transform of psi, consumed by the first graph step
@@ -955,6 +998,17 @@ int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
         // materialise the pending normalisation of the last step (stepper.cpp:67)
         dispatch(p, [&](auto r) { Launch<decltype(r)>::scale(p, field, -1, st->ds, true); });
     }
+}
+
+int gp5cu_stepper_advance(gp5cu_stepper *st, void *field, int nsteps) {
+    GP5_TRY
+    require(st != nullptr, "stepper is NULL");
+    check_field_ptr(field, "field");
+    require(nsteps >= 0, "nsteps must be >= 0");
+    gp5cu_plan *p = st->func->plan;
+    use_device(p);
+    if (nsteps == 0) return GP5_OK;
+    enqueue_advance(st, field, nsteps);
     sync_and_check(p, st->ds);
     GP5_CATCH
 }
@@ -990,6 +1044,56 @@ int gp5cu_stepper_advance_host(gp5cu_stepper *st, const void *host_in, void *hos
     if (rc != GP5_OK) return rc;
     check_cuda(cudaMemcpyAsync(host_out, st->dstate, p->field_bytes, cudaMemcpyDeviceToHost, p->stream), "download");
     check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    GP5_CATCH
+}
+
+int gp5cu_stepper_advance_host_many(gp5cu_stepper *st, int nstates, const void *const *host_in,
+                                    void *const *host_out, int nsteps) {
+    GP5_TRY
+    require(st && host_in && host_out, "NULL argument");
+    require(nstates >= 0 && nsteps >= 0, "nstates and nsteps must be >= 0");
+    for (int i = 0; i < nstates; i++) require(host_in[i] && host_out[i], "NULL host buffer");
+    gp5cu_plan *p = st->func->plan;
+    require(p->nsolve == 1, "host-buffer stepping needs a single-solve plan");
+    use_device(p);
+    if (nstates == 0) return GP5_OK;
+    const size_t fb = p->field_bytes;
+    if (!st->dstate) check_cuda(cudaMalloc(&st->dstate, fb), "cudaMalloc state");
+    if (!st->dstate2) check_cuda(cudaMalloc(&st->dstate2, fb), "cudaMalloc state");
+    if (!st->up) {
+        check_cuda(cudaStreamCreateWithFlags(&st->up, cudaStreamNonBlocking), "cudaStreamCreate");
+        check_cuda(cudaStreamCreateWithFlags(&st->down, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (int b = 0; b < 2; b++) {
+            check_cuda(cudaEventCreateWithFlags(&st->ev_up[b], cudaEventDisableTiming), "cudaEventCreate");
+            check_cuda(cudaEventCreateWithFlags(&st->ev_done[b], cudaEventDisableTiming), "cudaEventCreate");
+            check_cuda(cudaEventCreateWithFlags(&st->ev_down[b], cudaEventDisableTiming), "cudaEventCreate");
+        }
+    }
+    void *dbuf[2] = {st->dstate, st->dstate2};
+    // the plan stream's earlier work (for example the last call's steps) comes first
+    check_cuda(cudaEventRecord(st->ev_done[0], p->stream), "cudaEventRecord");
+    check_cuda(cudaStreamWaitEvent(st->up, st->ev_done[0], 0), "cudaStreamWaitEvent");
+    double t_after = st->t;
+    for (int i = 0; i < nstates; i++) {
+        const int b = i & 1;
+        // buffer b is free once state i-2 has been downloaded from it
+        if (i >= 2) check_cuda(cudaStreamWaitEvent(st->up, st->ev_down[b], 0), "cudaStreamWaitEvent");
+        check_cuda(cudaMemcpyAsync(dbuf[b], host_in[i], fb, cudaMemcpyHostToDevice, st->up), "upload");
+        check_cuda(cudaEventRecord(st->ev_up[b], st->up), "cudaEventRecord");
+        check_cuda(cudaStreamWaitEvent(p->stream, st->ev_up[b], 0), "cudaStreamWaitEvent");
+        st->comp_field = nullptr;  // a new state: its compensation starts from zero
+        const double t0 = st->t;
+        if (nsteps > 0) enqueue_advance(st, dbuf[b], nsteps);
+        if (i == 0) t_after = st->t;
+        st->t = t0;
+        check_cuda(cudaEventRecord(st->ev_done[b], p->stream), "cudaEventRecord");
+        check_cuda(cudaStreamWaitEvent(st->down, st->ev_done[b], 0), "cudaStreamWaitEvent");
+        check_cuda(cudaMemcpyAsync(host_out[i], dbuf[b], fb, cudaMemcpyDeviceToHost, st->down), "download");
+        check_cuda(cudaEventRecord(st->ev_down[b], st->down), "cudaEventRecord");
+    }
+    check_cuda(cudaStreamSynchronize(st->down), "sync");
+    sync_and_check(p, st->ds);
+    st->t = t_after;  // the states are independent: the stepper's time advances once
     GP5_CATCH
 }
 

@@ -41,7 +41,10 @@ inline TileGeom make_geom(const gp5cu_plan *p, int axis, int lines, bool pow2_bx
         g.lines = bx * bo;
         g.bx = bx;
         g.bo = bo;
-        g.tiles_x = (g.nx + bx - 1) / bx;
+        // the plan's x range (a slab of consecutive x values, or all of them)
+        g.x0 = p->xr_n > 0 ? p->xr0 : 0;
+        g.xend = p->xr_n > 0 ? p->xr0 + p->xr_n : g.nx;
+        g.tiles_x = (g.xend - g.x0 + bx - 1) / bx;
         g.n_other = axis == 1 ? (long long)g.nz * g.nc : (long long)g.ny * g.nc;
         tps = (long long)g.tiles_x * ((g.n_other + bo - 1) / bo);
     }
@@ -90,6 +93,7 @@ void launch_reg_th(gp5cu_plan *p, int axis, const Op &op) {
     constexpr int LINES = RegTile<Real, N, CONTIG, MODE, TH>::LINES, THREADS = RegTile<Real, N, CONTIG, MODE, TH>::THREADS;
     long long tiles = 0;
     TileGeom g = make_geom(p, axis, LINES, true, &tiles);
+    g.reverse = (MODE == MODE_INV_TURN_FWD && p->l2_order) ? 1 : 0;
     const size_t smem = CONTIG ? (size_t)LINES * LayContig<N>::LD * sizeof(V) : (size_t)LINES * N * sizeof(V);
     auto kern = k_axis_reg<Real, N, CONTIG, MODE, Op, TH>;
     ensure_smem(kern, smem, p->dev);
@@ -480,12 +484,25 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
         Launch<Real>::prologue(st, field);
         launches++;
     }
+    // The y forward, z (forward * K^2 * inverse) and y inverse passes run on slabs of
+    // consecutive x values, one slab after the other (p->yz_slabs of them): a slab's field
+    // stays in L2 from its y forward pass to its y inverse pass, so only the first reads and
+    // the last writes it in HBM.
+    const int slabs = std::max(1, p->yz_slabs);
+    const int sw = p->shape[0] / slabs;
     for (int s = 1; s <= nst; s++) {
         OpCopy<Real> cp{W, W, p->nsolve > 1 ? st->sp : nullptr};  // only a batch needs the active flags
-        launch_axis<Real, false, MODE_FWD>(p, 1, cp);
         OpKinetic<Real> kin{W, W, st->sp, p->shape[0], p->shape[1], p->shape[2]};
-        launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
-        launch_axis<Real, false, MODE_INV>(p, 1, cp);
+        for (int b = 0; b < slabs; b++) {
+            if (slabs > 1) {
+                p->xr0 = b * sw;
+                p->xr_n = sw;
+            }
+            launch_axis<Real, false, MODE_FWD>(p, 1, cp);
+            launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, kin);
+            launch_axis<Real, false, MODE_INV>(p, 1, cp);
+        }
+        p->xr0 = p->xr_n = 0;
         EpiParams<Real> P = base_epi<Real>(f);
         P.sp = st->sp;
         P.ds = st->ds;
@@ -497,6 +514,7 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
         P.slot = s & 1;
         P.u1_raw = (s == 1) ? 1 : 0;
         P.turn = 1;
+        P.stream_aux = p->stream_aux ? 1 : 0;
         P.renorm_out = st->renorm ? 1 : 0;
         P.phase_exp = nullptr;
         P.comp = nullptr;
@@ -522,7 +540,7 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
             OpStageOut<Real, false, true> op{W, P};
             launch_axis<Real, true, MODE_INV_TURN_FWD>(p, 0, op);
         }
-        launches += 4;
+        launches += 1 + 3 * slabs;
     }
     return launches;
 }

@@ -270,6 +270,7 @@ template <typename Real> struct EpiParams {
     double cfac;    // stage coefficient c = tau * cfac of u~ = sigma psi - c kprev
     double dfac;    // d = tau * dfac: tau (Euler) or tau/6 (RK4)
     int turn;       // also form the next stage's transform input (stage boundary kernel)
+    int stream_aux; // psi / k loads and stores with evict-first cache hints (read once per stage)
     double cnfac;   // next stage: u~' = sigma psi - (tau cnfac) k_s (RK1..RK3); psi1 for RK4/Euler
     // functional
     int fkind;
@@ -371,12 +372,25 @@ template <typename Real> struct EpiIn {
     cpx<Real> psi, kprev, kacc, lo;
 };
 
+// store of a psi / k element: evict-first when P.stream_aux
+template <typename Real>
+__device__ __forceinline__ void aux_store(const EpiParams<Real> &P, cpx<Real> *dst, cpx<Real> v) {
+    if (P.stream_aux) __stcs(dst, v);
+    else *dst = v;
+}
+
 template <typename Real>
 __device__ __forceinline__ EpiIn<Real> epi_load(const EpiParams<Real> &P, long long g) {
     EpiIn<Real> in;
-    in.psi = P.psi[g];
-    in.kprev = P.mode >= EPI_RK2 ? P.kprev[g] : mk<Real>(0, 0);
-    in.kacc = (P.mode == EPI_RK3 || P.mode == EPI_RK4) ? P.kacc[g] : mk<Real>(0, 0);
+    if (P.stream_aux) {
+        in.psi = __ldcs(P.psi + g);
+        in.kprev = P.mode >= EPI_RK2 ? __ldcs(P.kprev + g) : mk<Real>(0, 0);
+        in.kacc = (P.mode == EPI_RK3 || P.mode == EPI_RK4) ? __ldcs(P.kacc + g) : mk<Real>(0, 0);
+    } else {
+        in.psi = P.psi[g];
+        in.kprev = P.mode >= EPI_RK2 ? P.kprev[g] : mk<Real>(0, 0);
+        in.kacc = (P.mode == EPI_RK3 || P.mode == EPI_RK4) ? P.kacc[g] : mk<Real>(0, 0);
+    }
     if (P.comp && (P.mode == EPI_RK4 || P.mode == EPI_EULER)) {
         const float2 f = __bfloat1622float2(P.comp[g]);
         in.lo = mk<Real>((Real)f.x, (Real)f.y);
@@ -452,13 +466,13 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
         for (int c = 0; c < NC; c++) {
             const long long g = s + (long long)c * P.nsites;
             if (mode == EPI_RK1) {
-                P.kout[g] = h[c];
+                aux_store(P, P.kout + g, h[c]);
             } else if (mode == EPI_RK2) {
-                P.kout[g] = h[c];
-                P.kacc[g] = cadd(in[c].kprev, cscale(h[c], (Real)2));
+                aux_store(P, P.kout + g, h[c]);
+                aux_store(P, P.kacc + g, cadd(in[c].kprev, cscale(h[c], (Real)2)));
             } else {
-                P.kacc[g] = cadd(in[c].kacc, cscale(h[c], (Real)2));
-                P.kout[g] = h[c];
+                aux_store(P, P.kacc + g, cadd(in[c].kacc, cscale(h[c], (Real)2)));
+                aux_store(P, P.kout + g, h[c]);
             }
             if (TURN) {
                 V cn;
@@ -496,7 +510,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
             const Real a = sqrt(r.x * r.x + r.y * r.y);
             r = cscale(P.phase_exp[g], a);
         }
-        P.psi_out[g] = r;
+        aux_store(P, P.psi_out + g, r);
         if (TURN) next[c] = r;
         if (RED && P.renorm_out) acc[c] += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
     }

@@ -38,6 +38,8 @@ struct TileGeom {
     int nsolve;                 // independent solves of this grid in the launch
     long long tiles_per_solve;  // tiles of one solve (consecutive tile indices)
     long long solve_stride;     // elements between the fields of consecutive solves
+    int reverse;                // CTAs take the tiles from the last one down (L2 reuse order)
+    int x0, xend;               // strided passes: the x range [x0, xend) the tiles cover
 };
 
 struct RedSlot {
@@ -70,9 +72,9 @@ __device__ __forceinline__ LineRef line_ref(const TileGeom &g, long long tile_al
     } else {
         const long long tx = tile % g.tiles_x, to = tile / g.tiles_x;
         const int xo = line % g.bx, oo = line / g.bx;
-        int i = (int)(tx * g.bx) + xo;
+        int i = g.x0 + (int)(tx * g.bx) + xo;
         long long o = to * g.bo + oo;
-        r.valid = (i < g.nx) && (o < g.n_other);
+        r.valid = (i < g.xend) && (o < g.n_other);
         if (!r.valid) { i = 0; o = 0; }
         r.i = i;
         if (g.axis == 1) {  // o = k + nz*c
@@ -226,7 +228,22 @@ template <typename Real, int N, bool CONTIG, int MODE, int TH = 0> struct RegTil
     // resident CTAs (64: 8 CTAs of 128 threads, at most 8 bytes of spill); the other passes
     // keep 80.  (A cap of 96 for the complex128 strided copies measured slower: it spills.)
     static constexpr bool STRIDED_COPY = (MODE == MODE_FWD || MODE == MODE_INV) && !CONTIG;
-    static constexpr int REGCAP = sizeof(Real) == 8 ? 128 : (STRIDED_COPY || MODE == MODE_INV_TURN_FWD ? 64 : 80);
+#ifndef GP5_C64_CAP_COPY
+#define GP5_C64_CAP_COPY 64
+#endif
+#ifndef GP5_C64_CAP_BOUNDARY
+#define GP5_C64_CAP_BOUNDARY 64
+#endif
+#ifndef GP5_C64_CAP_OTHER
+#define GP5_C64_CAP_OTHER 80
+#endif
+#ifndef GP5_C128_CAP
+#define GP5_C128_CAP 128
+#endif
+    static constexpr int REGCAP = sizeof(Real) == 8 ? GP5_C128_CAP
+                                                    : (STRIDED_COPY ? GP5_C64_CAP_COPY
+                                                                    : (MODE == MODE_INV_TURN_FWD ? GP5_C64_CAP_BOUNDARY
+                                                                                                 : GP5_C64_CAP_OTHER));
     static constexpr int MINB_RAW = (65536 / REGCAP) / THREADS;
     static constexpr int MINB = MINB_RAW > 0 ? MINB_RAW : 1;
 };
@@ -250,7 +267,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
 #pragma unroll
     for (int r = 0; r < (Op::NRED > 0 ? Op::NRED : 1); r++) acc[r] = 0.0;
 
-    const long long tile = blockIdx.x;
+    const long long tile = g.reverse ? (long long)gridDim.x - 1 - blockIdx.x : (long long)blockIdx.x;
     const int solve = (int)(tile / g.tiles_per_solve);
     __shared__ typename Op::Ctx X;
     const void *streams[4];
@@ -411,7 +428,7 @@ k_axis_smem(const TileGeom g, const LineSchedule ls, Op op, const cpx<Real> *__r
 #pragma unroll
     for (int r = 0; r < K; r++) acc[r] = 0.0;
 
-    const long long tile = blockIdx.x;
+    const long long tile = g.reverse ? (long long)gridDim.x - 1 - blockIdx.x : (long long)blockIdx.x;
     const int solve = (int)(tile / g.tiles_per_solve);
     __shared__ typename Op::Ctx X;
     load_ctx(X, op.params(), op.scalars(), solve);

@@ -84,6 +84,18 @@ struct gp5cu_plan {
     int tile_threads[3][4] = {};
     // launches of the stepper path use programmatic dependent launch (GP5_PDL=0 turns it off)
     bool pdl = true;
+    // the stage boundary takes its tiles in reverse order (GP5_L2ORDER): it then starts on the
+    // planes the y inverse pass wrote last, which are still in L2, and the next y forward pass
+    // starts on the planes the boundary wrote last
+    bool l2_order = false;
+    // the stage boundary reads and writes psi and the k buffers with evict-first cache hints
+    // (GP5_STREAM_AUX), so that they do not push the transform buffer out of L2
+    bool stream_aux = false;
+    // the merged RK step runs its y/z passes on this many slabs of consecutive x values
+    // (GP5_YZ_SLABS; 1: one launch per pass over the whole field)
+    int yz_slabs = 1;
+    // x range of the strided (y/z) launches being queued: [xr0, xr0 + xr_n), or all when 0
+    int xr0 = 0, xr_n = 0;
 };
 
 struct gp5cu_functional {
@@ -116,6 +128,17 @@ struct gp5cu_stepper {
     void *graph_field = nullptr;
     bool graph_merged = false;
     int graph_steps = 0;
+    // the graph of the previously stepped field (two states alternate in the pipelined
+    // host-buffer entry point without re-capturing)
+    cudaGraphExec_t exec_alt = nullptr;
+    void *graph_field_alt = nullptr;
+    bool graph_merged_alt = false;
+    int graph_steps_alt = 0;
+    // pipelined host-buffer entry point: a second device state, upload / download streams and
+    // their events (created on first use)
+    void *dstate2 = nullptr;
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t ev_up[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_down[2] = {nullptr, nullptr};
     double t = 0;
     int launches_per_step = 0;
 };
@@ -159,4 +182,5 @@ bool merged_path(const gp5cu_plan *p);
 void autotune_plan(gp5cu_plan *p, bool force);
 int queue_step(gp5cu_stepper *st, void *field, bool merged, bool prologue);
 void build_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps);
+void capture_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps);
 void drop_graph(gp5cu_stepper *st);

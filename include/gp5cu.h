@@ -175,6 +175,16 @@ int gp5cu_stepper_set_time(gp5cu_stepper *st, double t);
  * host_in and host_out may alias. */
 int gp5cu_stepper_advance_host(gp5cu_stepper *st, const void *host_in, void *host_out,
                                int nsteps);
+/* The same for nstates independent host states (an ensemble, or states a caller streams
+ * through the GPU): state i is uploaded from host_in[i], advanced nsteps steps and downloaded
+ * to host_out[i].  Two device states alternate, with uploads and downloads on their own
+ * streams, so the upload of state i+1 and the download of state i-1 overlap the steps of
+ * state i (pinned host buffers are needed for the copies to overlap).  host_in[i] and
+ * host_out[i] may alias; states that share an output buffer overwrite it in order.  The stepper's time
+ * advances by nsteps steps once.  Single-solve plans only.  No reference counterpart (the
+ * reference keeps one state per process). */
+int gp5cu_stepper_advance_host_many(gp5cu_stepper *st, int nstates, const void *const *host_in,
+                                    void *const *host_out, int nsteps);
 /* Kernel launches one step issues (for launch accounting). */
 int gp5cu_stepper_launches_per_step(const gp5cu_stepper *st);
 /* Diagnostics (no reference counterpart; the reference's "step"/"FFT" timers,
