@@ -272,60 +272,41 @@ class WarmStart:
 # ---- data from the batched solver -----------------------------------------------------------
 def solve_ground_states(params: Sequence[dict], grid, tol: float, chunk: int = 512,
                         check_every: int = 100, max_steps: int = 400000, precision: int = _abi.GP5_C128,
-                        starts=None, device: int = 0, seed: int = 0, keep=None,
-                        caps: Sequence[int] = (1000, 3000, 10000, 30000, 100000, 400000), progress=None):
+                        starts=None, device: int = 0, seed: int = 0, keep=None, progress=None,
+                        devices: Optional[Sequence[int]] = None):
     """Solves every parameter set with the batched solver from a Gaussian (or
     starts(p, n, index)) on grid(p) (an int or a function of p); returns (states, results)
     lists in the order of params, each state passed through keep(p, psi) when keep is given.
 
-    A converged solve stops costing arithmetic but still takes part in every launch of its
-    batch, so the solves run in rounds: round j advances every unconverged solve up to caps[j]
-    steps in total, and the next round re-batches only those still above tol (from their
-    current states; the trajectory is the same as one uninterrupted run, since the RK4 step
-    carries no state besides psi).  results[i]["steps"] counts all rounds; progress(cap, n)
-    is called before each round with the number of solves it advances."""
+    The solves go to the batched solver `chunk` at a time (gp5cu_batch_*), which takes
+    finished solves out of its launches at every convergence check, so slow solves cost only
+    their own work.  devices: GPUs of this process to spread each chunk over (the solves are
+    independent and exchange nothing); default [device].  progress(done, total) is called
+    before each chunk."""
     count = len(params)
     gridof = (lambda p: grid(p)) if callable(grid) else (lambda p: int(grid))
     descs = [solve_desc(p, gridof(p)) for p in params]
-    done_steps = [0] * count
-    current = {}
+    devs = list(devices) if devices is not None else [device]
     states, results = [None] * count, [None] * count
-    pending = list(range(count))
-    caps = sorted({min(int(c), max_steps) for c in caps} | {max_steps})
-    for cap in caps:
-        if not pending:
-            break
+    for c0 in range(0, count, chunk):
+        part = list(range(c0, min(count, c0 + chunk)))
         if progress is not None:
-            progress(cap, len(pending))
-        still = []
-        for c0 in range(0, len(pending), chunk):
-            part = pending[c0:c0 + chunk]
-            b = _abi.Batch([descs[i] for i in part], precision=precision, device=device)
-            try:
-                for k, i in enumerate(part):
-                    if i in current:
-                        psi = current.pop(i)
-                    elif starts is not None:
-                        psi = starts(params[i], descs[i]["n"], i)
-                    else:
-                        psi = gaussian_start(params[i]["N"], descs[i]["n"], seed + i)
-                    b.set_state(k, psi)
-                budget = cap - max(done_steps[i] for i in part)
-                res = b.solve(tol=tol, check_every=check_every, max_steps=max(budget, check_every))
-                for k, i in enumerate(part):
-                    done_steps[i] += res[k]["steps"]
-                    r = dict(res[k])
-                    r["steps"] = done_steps[i]
-                    psi = b.get_state(k)[..., 0]
-                    if r["converged"] or cap >= max_steps:
-                        results[i] = r
-                        states[i] = keep(params[i], psi) if keep is not None else psi
-                    else:
-                        current[i] = np.asfortranarray(psi)
-                        still.append(i)
-            finally:
-                b.close()
-        pending = still
+            progress(c0, count)
+        b = _abi.Batch([descs[i] for i in part], precision=precision, devices=devs)
+        try:
+            for k, i in enumerate(part):
+                if starts is not None:
+                    psi = starts(params[i], descs[i]["n"], i)
+                else:
+                    psi = gaussian_start(params[i]["N"], descs[i]["n"], seed + i)
+                b.set_state(k, psi)
+            res = b.solve(tol=tol, check_every=check_every, max_steps=max_steps)
+            for k, i in enumerate(part):
+                results[i] = dict(res[k])
+                psi = b.get_state(k)[..., 0]
+                states[i] = keep(params[i], psi) if keep is not None else psi
+        finally:
+            b.close()
     return states, results
 
 
@@ -339,20 +320,20 @@ def training_grid(p: dict) -> int:
 
 
 def make_training_set(count: int = 4096, seed: int = TRAIN_SEED, grid=training_grid, tol: float = 1e-7,
-                      chunk: int = 1024, device: int = 0):
+                      chunk: int = 1024, device: int = 0, devices: Optional[Sequence[int]] = None):
     """Ground states of `count` seeded parameter sets (batched imaginary-time RK4 in complex128
-    from the noise-free Gaussian, to residual tol, on grid(p)^3); returns (params, radial
-    samples [count][64], solver results)."""
+    from the noise-free Gaussian, to residual tol, on grid(p)^3), spread over `devices` when
+    given; returns (params, radial samples [count][64], solver results)."""
     params = sample_params(count, seed)
     keep = lambda p, psi: radial_samples(psi, p["N"])
     import sys
     import time
 
     t0 = time.time()
-    report = lambda cap, k: print(f"[{time.time() - t0:7.1f} s] round to {cap} steps: {k} solves",
-                                  file=sys.stderr, flush=True)
+    report = lambda done, total: print(f"[{time.time() - t0:7.1f} s] {done} of {total} solves done",
+                                       file=sys.stderr, flush=True)
     samples, results = solve_ground_states(params, grid, tol=tol, chunk=chunk, device=device, keep=keep,
-                                           progress=report,
+                                           progress=report, devices=devices,
                                            starts=lambda p, n, k: gaussian_start(p["N"], n, None))
     return params, np.asarray(samples), results
 
@@ -369,8 +350,8 @@ def evaluate(model: "WarmStart", count: int = 64, seed: int = TEST_SEED, n: int 
     pred = model.predict(params)
     keep = lambda p, psi: radial_samples(psi, p["N"])
     t0 = time.time()
-    report = lambda cap, k: print(f"[{time.time() - t0:7.1f} s] round to {cap} steps: {k} solves",
-                                  file=sys.stderr, flush=True)
+    report = lambda done, total: print(f"[{time.time() - t0:7.1f} s] {done} of {total} solves done",
+                                       file=sys.stderr, flush=True)
     sg, rg = solve_ground_states(params, n, tol=tol, chunk=count, check_every=check_every, device=device,
                                  keep=keep, progress=report,
                                  starts=lambda p, m, k: gaussian_start(p["N"], m, None))
@@ -415,6 +396,8 @@ def main(argv=None):
     ap.add_argument("--data", metavar="NPZ", help="reuse (or save) the training set here")
     ap.add_argument("--test-count", type=int, default=64)
     ap.add_argument("--test-grid", type=int, default=128)
+    ap.add_argument("--devices", type=int, nargs="+", default=None,
+                    help="GPUs to spread the training-set solves over (independent solves)")
     a = ap.parse_args(argv)
     if a.train:
         t0 = time.time()
@@ -423,7 +406,7 @@ def main(argv=None):
             params = [dict(N=float(r[0]), c3=float(r[1]), omega=float(r[2])) for r in z["params"]]
             samples, steps = z["samples"].astype(np.float64), z["steps"]
         else:
-            params, samples, results = make_training_set(a.count)
+            params, samples, results = make_training_set(a.count, devices=a.devices)
             steps = np.array([r["steps"] for r in results])
             if a.data:
                 table = np.array([[p["N"], p["c3"], p["omega"]] for p in params])

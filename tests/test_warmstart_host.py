@@ -1,4 +1,4 @@
-"""Host-side logic of the warm start (no GPU): re-batching of unconverged solves and the
+"""Host-side logic of the warm start (no GPU): the chunked ground-state driver and the
 periodic image-sum placement of radial samples."""
 import math
 
@@ -12,7 +12,7 @@ class FakeBatch:
     need = {}
     created = []
 
-    def __init__(self, descs, precision=0, device=0):
+    def __init__(self, descs, precision=0, device=0, devices=None):
         self.descs = descs
         self.states = [None] * len(descs)
         FakeBatch.created.append(len(descs))
@@ -41,28 +41,29 @@ class FakeBatch:
         pass
 
 
-def test_rebatching_counts_steps_and_keeps_order(monkeypatch):
+def test_chunks_count_steps_and_keep_order(monkeypatch):
+    """Each chunk goes to one batch (the batched solver takes finished solves out of its
+    launches itself); results come back in the order of params."""
     params = [dict(N=float(20 + k), c3=-3.0, omega=0.0) for k in range(7)]
     FakeBatch.need = {p["N"]: s for p, s in zip(params, [300, 5000, 900, 45000, 100, 2500, 12000])}
     FakeBatch.created = []
     monkeypatch.setattr(ws._abi, "Batch", FakeBatch)
     starts = lambda p, n, i: np.zeros((4, 4, 4), complex)
     states, res = ws.solve_ground_states(params, 4, tol=1e-8, chunk=3, starts=starts, check_every=100,
-                                         caps=(1000, 3000, 10000, 30000, 100000), max_steps=100000)
+                                         max_steps=100000, devices=[0, 1])
     assert [r["steps"] for r in res] == [300, 5000, 900, 45000, 100, 2500, 12000]
     assert all(r["converged"] for r in res)
     assert [r["energy"] for r in res] == [-p["N"] for p in params]
-    # round sizes: 7 solves (chunks 3,3,1), then 4 above 1000 steps, 3 above 3000, 2, 1
-    assert FakeBatch.created == [3, 3, 1, 3, 1, 3, 2, 1]
+    assert FakeBatch.created == [3, 3, 1]
 
 
-def test_rebatching_reports_unconverged_at_max_steps(monkeypatch):
+def test_unconverged_at_max_steps(monkeypatch):
     params = [dict(N=21.0, c3=-3.0, omega=0.0), dict(N=22.0, c3=-3.0, omega=0.0)]
     FakeBatch.need = {21.0: 700, 22.0: 10 ** 9}
     FakeBatch.created = []
     monkeypatch.setattr(ws._abi, "Batch", FakeBatch)
     starts = lambda p, n, i: np.zeros((4, 4, 4), complex)
-    _, res = ws.solve_ground_states(params, 4, tol=1e-8, starts=starts, caps=(1000,), max_steps=4000)
+    _, res = ws.solve_ground_states(params, 4, tol=1e-8, starts=starts, max_steps=4000)
     assert res[0]["steps"] == 700 and res[0]["converged"]
     assert res[1]["steps"] == 4000 and not res[1]["converged"]
 
