@@ -148,6 +148,8 @@ def lib():
         "gp5cu_plan_autotune": (i, [vp]),
         "gp5cu_plan_get_tiles": (i, [vp, C.POINTER(C.c_int)]),
         "gp5cu_plan_set_tiles": (i, [vp, C.POINTER(C.c_int)]),
+        "gp5cu_plan_get_radix": (i, [vp, C.POINTER(C.c_int)]),
+        "gp5cu_plan_set_radix": (i, [vp, C.POINTER(C.c_int)]),
         "gp5cu_mlp_create": (i, [pp, i, C.c_ulonglong]),
         "gp5cu_mlp_destroy": (i, [vp]),
         "gp5cu_mlp_num_params": (C.c_longlong, [vp]),
@@ -249,6 +251,16 @@ class Plan:
     def set_tiles(self, threads) -> None:
         t = (C.c_int * 5)(*[int(v) for v in threads])
         check(lib().gp5cu_plan_set_tiles(self.h, t))
+
+    def radix(self):
+        """Radix schedules (0/1) of (y fwd, y inv, z fwd, z inv, z fwd*K^2*inv, x stage boundary)."""
+        r = (C.c_int * 6)()
+        check(lib().gp5cu_plan_get_radix(self.h, r))
+        return list(r)
+
+    def set_radix(self, radix) -> None:
+        r = (C.c_int * 6)(*[int(v) for v in radix])
+        check(lib().gp5cu_plan_set_radix(self.h, r))
 
     def autotune(self) -> None:
         check(lib().gp5cu_plan_autotune(self.h))

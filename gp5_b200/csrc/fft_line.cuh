@@ -165,40 +165,55 @@ template <int DIR, typename V> __device__ __forceinline__ V twiddle(const V *__r
 }
 
 // ------------------------------------------------------------------------------------------
-// register engine: N = 2^p, radix schedule fixed at compile time
+// register engine: N = 2^p, radix schedule fixed at compile time.  Two schedules per length:
+// S = 0 and S = 1 differ in the elements a thread owns (E) and so in the threads per line
+// (N / E), the passes and the registers a thread needs; the plan's autotuner picks one per
+// pass.  The two round differently (other butterflies, other twiddle products), so a plan
+// keeps its choice for every plan of the same grid and precision (see autotune_plan).
 // ------------------------------------------------------------------------------------------
-template <int N> struct RegCfg;
-template <> struct RegCfg<16> { static constexpr int E = 4, NP = 2; static constexpr int rad(int p) { return 4; } };
-template <> struct RegCfg<32> { static constexpr int E = 8, NP = 2; static constexpr int rad(int p) { return p == 0 ? 8 : 4; } };
-template <> struct RegCfg<64> { static constexpr int E = 8, NP = 2; static constexpr int rad(int p) { return 8; } };
-template <> struct RegCfg<128> { static constexpr int E = 16, NP = 2; static constexpr int rad(int p) { return p == 0 ? 16 : 8; } };
-template <> struct RegCfg<256> { static constexpr int E = 16, NP = 2; static constexpr int rad(int p) { return 16; } };
-template <> struct RegCfg<512> { static constexpr int E = 8, NP = 3; static constexpr int rad(int p) { return 8; } };
-template <> struct RegCfg<1024> { static constexpr int E = 16, NP = 3; static constexpr int rad(int p) { return p == 2 ? 4 : 16; } };
+template <int N, int S = 0> struct RegCfg;
+template <> struct RegCfg<16, 0> { static constexpr int E = 4, NP = 2; static constexpr int rad(int p) { return 4; } };
+template <> struct RegCfg<32, 0> { static constexpr int E = 8, NP = 2; static constexpr int rad(int p) { return p == 0 ? 8 : 4; } };
+template <> struct RegCfg<64, 0> { static constexpr int E = 8, NP = 2; static constexpr int rad(int p) { return 8; } };
+template <> struct RegCfg<128, 0> { static constexpr int E = 16, NP = 2; static constexpr int rad(int p) { return p == 0 ? 16 : 8; } };
+template <> struct RegCfg<256, 0> { static constexpr int E = 16, NP = 2; static constexpr int rad(int p) { return 16; } };
+template <> struct RegCfg<512, 0> { static constexpr int E = 8, NP = 3; static constexpr int rad(int p) { return 8; } };
+template <> struct RegCfg<1024, 0> { static constexpr int E = 16, NP = 3; static constexpr int rad(int p) { return p == 2 ? 4 : 16; } };
+// S = 1: half the elements per thread (twice the threads per line, fewer registers), except
+// 512 (twice the elements: radix-16 passes)
+template <> struct RegCfg<16, 1> : RegCfg<16, 0> {};
+template <> struct RegCfg<32, 1> { static constexpr int E = 4, NP = 3; static constexpr int rad(int p) { return p == 2 ? 2 : 4; } };
+template <> struct RegCfg<64, 1> { static constexpr int E = 4, NP = 3; static constexpr int rad(int p) { return 4; } };
+template <> struct RegCfg<128, 1> { static constexpr int E = 8, NP = 3; static constexpr int rad(int p) { return p == 2 ? 2 : 8; } };
+template <> struct RegCfg<256, 1> { static constexpr int E = 8, NP = 3; static constexpr int rad(int p) { return p == 2 ? 4 : 8; } };
+template <> struct RegCfg<512, 1> { static constexpr int E = 16, NP = 3; static constexpr int rad(int p) { return p == 2 ? 2 : 16; } };
+template <> struct RegCfg<1024, 1> : RegCfg<1024, 0> {};
 
-template <int N> struct RegCfgAll : RegCfg<N> {
-    static constexpr int T = N / RegCfg<N>::E;
-    static constexpr int ns(int p) { return p == 0 ? 1 : ns(p - 1) * RegCfg<N>::rad(p - 1); }
+template <int N, int S = 0> struct RegCfgAll : RegCfg<N, S> {
+    static constexpr int T = N / RegCfg<N, S>::E;
+    static constexpr int ns(int p) { return p == 0 ? 1 : ns(p - 1) * RegCfg<N, S>::rad(p - 1); }
 };
 
 // Shared-memory index maps for the exchange between passes.
 //  * strided-axis tiles: element (line, pos) at pos*LINES + line (lanes run over lines)
-//  * x-axis tiles: element (line, pos) at line*LD + pos + pos/16 (one pad slot every 16
-//    elements so that the stride-16 scatter of a radix-16 pass spreads over the banks)
+//  * x-axis tiles: element (line, pos) at line*LD + pos + pos/P, one pad slot every P elements
+//    (P = 16, or the first pass's radix for S = 1) so that the stride-P scatter of the first
+//    pass spreads over the banks
 struct LayStrided {
     int lines;
     __device__ __forceinline__ int operator()(int line, int pos) const { return pos * lines + line; }
 };
-template <int N> struct LayContig {
-    static constexpr int LD = N + N / 16 + 1;
-    __device__ __forceinline__ int operator()(int line, int pos) const { return line * LD + pos + (pos >> 4); }
+template <int N, int S = 0> struct LayContig {
+    static constexpr int P = S == 0 ? 16 : RegCfg<N, S>::rad(0);
+    static constexpr int LD = N + N / P + 1;
+    __device__ __forceinline__ int operator()(int line, int pos) const { return line * LD + pos + pos / P; }
 };
 
 // One Stockham pass P of the register engine on the E registers of one line-thread.
-template <int N, int P, int DIR, typename V, class Lay>
-__device__ __forceinline__ void reg_pass(V (&v)[RegCfg<N>::E], int tid, int line,
+template <int N, int S, int P, int DIR, typename V, class Lay>
+__device__ __forceinline__ void reg_pass(V (&v)[RegCfg<N, S>::E], int tid, int line,
                                          const V *__restrict__ tw, V *sm, const Lay &lay) {
-    using C = RegCfgAll<N>;
+    using C = RegCfgAll<N, S>;
     constexpr int E = C::E, T = C::T, R = C::rad(P), Ns = C::ns(P);
     constexpr bool last = (P == C::NP - 1);
 #pragma unroll
@@ -254,20 +269,20 @@ __device__ __forceinline__ void reg_pass(V (&v)[RegCfg<N>::E], int tid, int line
     }
 }
 
-template <int N, int P, int DIR, typename V, class Lay>
-__device__ __forceinline__ void reg_fft_from(V (&v)[RegCfg<N>::E], int tid, int line,
+template <int N, int S, int P, int DIR, typename V, class Lay>
+__device__ __forceinline__ void reg_fft_from(V (&v)[RegCfg<N, S>::E], int tid, int line,
                                              const V *__restrict__ tw, V *sm, const Lay &lay) {
-    if constexpr (P < RegCfg<N>::NP) {
-        reg_pass<N, P, DIR>(v, tid, line, tw, sm, lay);
-        reg_fft_from<N, P + 1, DIR>(v, tid, line, tw, sm, lay);
+    if constexpr (P < RegCfg<N, S>::NP) {
+        reg_pass<N, S, P, DIR>(v, tid, line, tw, sm, lay);
+        reg_fft_from<N, S, P + 1, DIR>(v, tid, line, tw, sm, lay);
     }
 }
 
-// Full length-N transform of the line held in v (positions tid + T*m in, and out).
-template <int N, int DIR, typename V, class Lay>
-__device__ __forceinline__ void reg_fft(V (&v)[RegCfg<N>::E], int tid, int line,
+// Full length-N transform of the line held in v (positions tid + T*m in, and out), schedule S.
+template <int N, int S, int DIR, typename V, class Lay>
+__device__ __forceinline__ void reg_fft(V (&v)[RegCfg<N, S>::E], int tid, int line,
                                         const V *__restrict__ tw, V *sm, const Lay &lay) {
-    reg_fft_from<N, 0, DIR>(v, tid, line, tw, sm, lay);
+    reg_fft_from<N, S, 0, DIR>(v, tid, line, tw, sm, lay);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -125,12 +125,12 @@ void build_axis_plan(gp5cu_plan *p, int d) {
     ap.n = n;
     ap.reg = (n == 32 || n == 64 || n == 128 || n == 256 || n == 512);
     switch (n) {
-        case 32: ap.reg_threads = RegCfgAll<32>::T; break;
-        case 64: ap.reg_threads = RegCfgAll<64>::T; break;
-        case 128: ap.reg_threads = RegCfgAll<128>::T; break;
-        case 256: ap.reg_threads = RegCfgAll<256>::T; break;
-        case 512: ap.reg_threads = RegCfgAll<512>::T; break;
-        default: ap.reg_threads = 0;
+        case 32: ap.reg_threads = RegCfgAll<32>::T, ap.reg_threads1 = RegCfgAll<32, 1>::T; break;
+        case 64: ap.reg_threads = RegCfgAll<64>::T, ap.reg_threads1 = RegCfgAll<64, 1>::T; break;
+        case 128: ap.reg_threads = RegCfgAll<128>::T, ap.reg_threads1 = RegCfgAll<128, 1>::T; break;
+        case 256: ap.reg_threads = RegCfgAll<256>::T, ap.reg_threads1 = RegCfgAll<256, 1>::T; break;
+        case 512: ap.reg_threads = RegCfgAll<512>::T, ap.reg_threads1 = RegCfgAll<512, 1>::T; break;
+        default: ap.reg_threads = ap.reg_threads1 = 0;
     }
     if (!factorize(n, ap.sched))
         fail(GP5_ERR_UNSUPPORTED, "axis length " + std::to_string(n) + " has a prime factor > 61");
@@ -212,13 +212,21 @@ static SolveParams geometry_params(const int shape[3], const double left[3], con
 }
 
 // A plan for nsolve independent solves of one grid (boxes may differ per solve).
-// Tile shapes chosen by the autotuner, per (device model, shape, components, precision,
-// solves), kept in memory and in a JSON file: GP5_AUTOTUNE_CACHE names it (empty: no file),
-// default $XDG_CACHE_HOME/gp5_b200/autotune.json or ~/.cache/gp5_b200/autotune.json.  The file
-// maps "<device>|<nx>x<ny>x<nz>|c<ncomp>|<c128|c64>|s<nsolve>|build <date time>" to the five thread counts of
-// gp5cu_plan_get_tiles.  GP5_AUTOTUNE=0 keeps the default shapes.
+// Choices of the autotuner, kept in memory and in a JSON file: GP5_AUTOTUNE_CACHE names it
+// (empty: no file), default $XDG_CACHE_HOME/gp5_b200/autotune.json or
+// ~/.cache/gp5_b200/autotune.json.  Two kinds of entries:
+//   "radix|<device>|<nx>x<ny>x<nz>|c<ncomp>|<c128|c64>|build <date time>": the radix schedule
+//     (0/1) of the five tuned passes of gp5cu_plan_get_tiles and of the stage boundary.  The
+//     schedules round differently, so they are chosen once per grid and precision and every
+//     plan of that grid uses them, whatever its number of solves (a batch is then bitwise a
+//     set of single solves);
+//   "<device>|<nx>x<ny>x<nz>|c<ncomp>|<c128|c64>|s<nsolve>|r<radices>|build <date time>": the
+//     five thread counts of gp5cu_plan_get_tiles for those schedules (they change no result
+//     bit).
+// GP5_AUTOTUNE=0 keeps the default shapes and schedule 0; GP5_RADIX=0 or 1 fixes the schedule
+// of every tuned pass and of the boundary (the thread counts are still tuned).
 static std::mutex g_tune_mu;
-static std::map<std::string, std::array<int, kTunedPasses>> g_tune_cache;
+static std::map<std::string, std::vector<int>> g_tune_cache;
 static bool g_tune_loaded = false;
 
 static std::string tune_cache_path() {
@@ -231,7 +239,7 @@ static std::string tune_cache_path() {
     return std::string();
 }
 
-// reads entries "key": [a, b, c, d, e]; anything else in the file is skipped
+// reads entries "key": [integers]; anything else in the file is skipped
 static void tune_cache_load(const std::string &path) {
     FILE *f = path.empty() ? nullptr : std::fopen(path.c_str(), "rb");
     if (!f) return;
@@ -250,19 +258,24 @@ static void tune_cache_load(const std::string &path) {
             pos = end + 1;
             continue;
         }
-        std::array<int, kTunedPasses> v{};
-        bool ok = true;
+        const size_t close = txt.find(']', q);
+        if (close == std::string::npos) break;
+        std::vector<int> v;
         const char *c = txt.c_str() + q + 1;
-        for (int t = 0; t < kTunedPasses && ok; t++) {
+        const char *stop = txt.c_str() + close;
+        while (c < stop) {
             char *next = nullptr;
             const long x = std::strtol(c, &next, 10);
-            if (next == c || !(x == 0 || x == 128 || x == 256 || x == 512)) ok = false;
-            v[t] = (int)x;
+            if (next == c) break;
+            v.push_back((int)x);
             c = next;
-            while (*c == ' ' || *c == ',' || *c == '\n' || *c == '\t' || *c == '\r') c++;
+            while (c < stop && (*c == ' ' || *c == ',' || *c == '\n' || *c == '\t' || *c == '\r')) c++;
         }
+        const bool is_radix = key.compare(0, 6, "radix|") == 0;
+        bool ok = (int)v.size() == (is_radix ? kTunedPasses + 1 : kTunedPasses);
+        for (int x : v) ok = ok && (is_radix ? (x == 0 || x == 1) : (x == 0 || x == 128 || x == 256 || x == 512));
         if (ok) g_tune_cache[key] = v;
-        pos = end + 1;
+        pos = close + 1;
     }
 }
 
@@ -279,24 +292,47 @@ static void tune_cache_store(const std::string &path) {
     std::fprintf(f, "{\n");
     size_t i = 0;
     for (const auto &kv : g_tune_cache) {
-        std::fprintf(f, "  \"%s\": [%d, %d, %d, %d, %d]%s\n", kv.first.c_str(), kv.second[0], kv.second[1],
-                     kv.second[2], kv.second[3], kv.second[4], ++i < g_tune_cache.size() ? "," : "");
+        std::fprintf(f, "  \"%s\": [", kv.first.c_str());
+        for (size_t k = 0; k < kv.second.size(); k++) std::fprintf(f, "%s%d", k ? ", " : "", kv.second[k]);
+        std::fprintf(f, "]%s\n", ++i < g_tune_cache.size() ? "," : "");
     }
     std::fprintf(f, "}\n");
     std::fclose(f);
     std::rename(tmp.c_str(), path.c_str());
 }
 
-static std::string tune_key(const gp5cu_plan *p) {
+static std::string grid_key(const gp5cu_plan *p) {
     cudaDeviceProp prop{};
     cudaGetDeviceProperties(&prop, p->dev);
     std::string name(prop.name);
     for (char &ch : name)
         if (ch == '"' || ch == '|' || ch == '\\') ch = '_';
     return name + "|" + std::to_string(p->shape[0]) + "x" + std::to_string(p->shape[1]) + "x" +
-           std::to_string(p->shape[2]) + "|c" + std::to_string(p->ncomp) + "|" +
-           (p->prec == GP5_C128 ? "c128" : "c64") + "|s" + std::to_string(p->nsolve) +
-           "|build " __DATE__ " " __TIME__;  // another build tunes afresh
+           std::to_string(p->shape[2]) + "|c" + std::to_string(p->ncomp) + "|" + (p->prec == GP5_C128 ? "c128" : "c64");
+}
+
+static const char *kBuildStamp = "|build " __DATE__ " " __TIME__;  // another build tunes afresh
+
+static std::vector<int> radix_vector(const gp5cu_plan *p) {
+    std::vector<int> v(kTunedPasses + 1);
+    for (int q = 0; q < kTunedPasses; q++) v[q] = p->radix[kTunedAxis[q]][kTunedMode[q]];
+    v[kTunedPasses] = p->radix_boundary;
+    return v;
+}
+
+static void apply_radix(gp5cu_plan *p, const std::vector<int> &v) {
+    for (int q = 0; q < kTunedPasses; q++) p->radix[kTunedAxis[q]][kTunedMode[q]] = p->ax[kTunedAxis[q]].reg ? v[q] : 0;
+    p->radix_boundary = p->ax[0].reg ? v[kTunedPasses] : 0;
+}
+
+static void apply_threads(gp5cu_plan *p, const std::vector<int> &v) {
+    for (int q = 0; q < kTunedPasses; q++) {
+        const int t = v[q];
+        const int axis = kTunedAxis[q];
+        const AxisPlan &ap = p->ax[axis];
+        const int T = p->radix[axis][kTunedMode[q]] == 0 ? ap.reg_threads : ap.reg_threads1;
+        p->tile_threads[axis][kTunedMode[q]] = (t != 0 && ap.reg && T > 0 && t % T == 0) ? t : 0;
+    }
 }
 
 void autotune_plan(gp5cu_plan *p, bool force) {
@@ -308,22 +344,40 @@ void autotune_plan(gp5cu_plan *p, bool force) {
         tune_cache_load(path);
         g_tune_loaded = true;
     }
-    const std::string key = tune_key(p);
-    auto it = g_tune_cache.find(key);
-    if (!force && it != g_tune_cache.end()) {
-        for (int q = 0; q < kTunedPasses; q++) {
-            const int t = it->second[q];
-            const AxisPlan &ap = p->ax[kTunedAxis[q]];
-            p->tile_threads[kTunedAxis[q]][kTunedMode[q]] = (t != 0 && ap.reg && t % ap.reg_threads == 0) ? t : 0;
+    const std::string rkey = "radix|" + grid_key(p) + kBuildStamp;
+    bool have_radix = false;
+    const char *fixed = std::getenv("GP5_RADIX");
+    if (fixed && (std::string(fixed) == "0" || std::string(fixed) == "1")) {
+        apply_radix(p, std::vector<int>(kTunedPasses + 1, std::atoi(fixed)));
+        have_radix = true;
+    } else {
+        // a forced re-tune times the thread counts again but keeps the grid's schedules, so
+        // that every plan of the grid keeps rounding the same way
+        auto it = g_tune_cache.find(rkey);
+        if (it != g_tune_cache.end()) {
+            apply_radix(p, it->second);
+            have_radix = true;
         }
-        return;
     }
-    if (p->prec == GP5_C128) Launch<double>::autotune(p, 3);
-    else Launch<float>::autotune(p, 3);
+    auto thread_key = [&] {
+        std::string r;
+        for (int x : radix_vector(p)) r += std::to_string(x);
+        return grid_key(p) + "|s" + std::to_string(p->nsolve) + "|r" + r + kBuildStamp;
+    };
+    if (have_radix && !force) {
+        auto it = g_tune_cache.find(thread_key());
+        if (it != g_tune_cache.end()) {
+            apply_threads(p, it->second);
+            return;
+        }
+    }
+    if (p->prec == GP5_C128) Launch<double>::autotune(p, 3, !have_radix);
+    else Launch<float>::autotune(p, 3, !have_radix);
     check_cuda(cudaStreamSynchronize(p->stream), "sync");
-    std::array<int, kTunedPasses> v{};
+    if (!have_radix) g_tune_cache[rkey] = radix_vector(p);
+    std::vector<int> v(kTunedPasses);
     for (int q = 0; q < kTunedPasses; q++) v[q] = p->tile_threads[kTunedAxis[q]][kTunedMode[q]];
-    g_tune_cache[key] = v;
+    g_tune_cache[thread_key()] = v;
     tune_cache_store(path);
 }
 
@@ -478,9 +532,35 @@ int gp5cu_plan_set_tiles(gp5cu_plan *p, const int threads[5]) {
         const int t = threads[q];
         require(t == 0 || t == 128 || t == 256 || t == 512, "tile threads must be 0, 128, 256 or 512");
         const AxisPlan &ap = p->ax[kTunedAxis[q]];
-        require(t == 0 || (ap.reg && t % ap.reg_threads == 0), "tile threads do not fit this axis");
+        const int T = p->radix[kTunedAxis[q]][kTunedMode[q]] == 0 ? ap.reg_threads : ap.reg_threads1;
+        require(t == 0 || (ap.reg && t % T == 0), "tile threads do not fit this axis");
     }
     for (int q = 0; q < kTunedPasses; q++) p->tile_threads[kTunedAxis[q]][kTunedMode[q]] = threads[q];
+    GP5_CATCH
+}
+
+int gp5cu_plan_get_radix(const gp5cu_plan *p, int radix[6]) {
+    GP5_TRY
+    require(p != nullptr && radix != nullptr, "NULL argument");
+    for (int q = 0; q < kTunedPasses; q++) radix[q] = p->radix[kTunedAxis[q]][kTunedMode[q]];
+    radix[kTunedPasses] = p->radix_boundary;
+    GP5_CATCH
+}
+
+int gp5cu_plan_set_radix(gp5cu_plan *p, const int radix[6]) {
+    GP5_TRY
+    require(p != nullptr && radix != nullptr, "NULL argument");
+    for (int q = 0; q <= kTunedPasses; q++) require(radix[q] == 0 || radix[q] == 1, "radix schedules are 0 or 1");
+    for (int q = 0; q < kTunedPasses; q++) {
+        const int axis = kTunedAxis[q], mode = kTunedMode[q];
+        const AxisPlan &ap = p->ax[axis];
+        p->radix[axis][mode] = ap.reg ? radix[q] : 0;
+        // a thread count that does not fit the new schedule falls back to the default shape
+        const int T = p->radix[axis][mode] == 0 ? ap.reg_threads : ap.reg_threads1;
+        if (p->tile_threads[axis][mode] != 0 && (T == 0 || p->tile_threads[axis][mode] % T != 0))
+            p->tile_threads[axis][mode] = 0;
+    }
+    p->radix_boundary = p->ax[0].reg ? radix[kTunedPasses] : 0;
     GP5_CATCH
 }
 

@@ -87,15 +87,16 @@ template <class K> inline void ensure_smem(K kernel, size_t bytes, int dev) {
     if (bytes > 48 * 1024) smem_opt_in((const void *)kernel, bytes, dev);
 }
 
-template <typename Real, int N, bool CONTIG, int MODE, class Op, int TH>
+template <typename Real, int N, bool CONTIG, int MODE, class Op, int TH, int S>
 void launch_reg_th(gp5cu_plan *p, int axis, const Op &op) {
     using V = cpx<Real>;
-    constexpr int LINES = RegTile<Real, N, CONTIG, MODE, TH>::LINES, THREADS = RegTile<Real, N, CONTIG, MODE, TH>::THREADS;
+    constexpr int LINES = RegTile<Real, N, CONTIG, MODE, TH, S>::LINES,
+                  THREADS = RegTile<Real, N, CONTIG, MODE, TH, S>::THREADS;
     long long tiles = 0;
     TileGeom g = make_geom(p, axis, LINES, true, &tiles);
     g.reverse = (MODE == MODE_INV_TURN_FWD && p->l2_order) ? 1 : 0;
-    const size_t smem = CONTIG ? (size_t)LINES * LayContig<N>::LD * sizeof(V) : (size_t)LINES * N * sizeof(V);
-    auto kern = k_axis_reg<Real, N, CONTIG, MODE, Op, TH>;
+    const size_t smem = CONTIG ? (size_t)LINES * LayContig<N, S>::LD * sizeof(V) : (size_t)LINES * N * sizeof(V);
+    auto kern = k_axis_reg<Real, N, CONTIG, MODE, Op, TH, S>;
     ensure_smem(kern, smem, p->dev);
     if (p->dry) return;
     launch_k(p, kern, (unsigned)tiles, THREADS, smem, g, op, (const V *)p->ax[axis].tw, red_slot(p));
@@ -103,20 +104,34 @@ void launch_reg_th(gp5cu_plan *p, int axis, const Op &op) {
 }
 
 // Tile shapes of the strided (y/z) passes: the plan's autotuned threads per CTA (0: the
-// default rule of RegTile).  These passes carry no reductions, so the choice does not change
-// any result bit.
-template <typename Real, int N, bool CONTIG, int MODE, class Op>
-void launch_reg(gp5cu_plan *p, int axis, const Op &op) {
+// default rule of RegTile).  These passes carry no reductions, so the thread count does not
+// change any result bit.
+template <typename Real, int N, bool CONTIG, int MODE, class Op, int S>
+void launch_reg_s(gp5cu_plan *p, int axis, const Op &op) {
     if constexpr (!CONTIG && (MODE == MODE_FWD || MODE == MODE_INV || MODE == MODE_FWD_MID_INV)) {
-        constexpr int T = RegCfgAll<N>::T, DEF = RegTile<Real, N, CONTIG, MODE, 0>::THREADS;
+        constexpr int T = RegCfgAll<N, S>::T, DEF = RegTile<Real, N, CONTIG, MODE, 0, S>::THREADS;
         switch (p->tile_threads[axis][MODE]) {
-            case 128: if constexpr (128 % T == 0 && DEF != 128) { launch_reg_th<Real, N, CONTIG, MODE, Op, 128>(p, axis, op); return; } break;
-            case 256: if constexpr (256 % T == 0 && DEF != 256) { launch_reg_th<Real, N, CONTIG, MODE, Op, 256>(p, axis, op); return; } break;
-            case 512: if constexpr (512 % T == 0 && DEF != 512) { launch_reg_th<Real, N, CONTIG, MODE, Op, 512>(p, axis, op); return; } break;
+            case 128: if constexpr (128 % T == 0 && DEF != 128) { launch_reg_th<Real, N, CONTIG, MODE, Op, 128, S>(p, axis, op); return; } break;
+            case 256: if constexpr (256 % T == 0 && DEF != 256) { launch_reg_th<Real, N, CONTIG, MODE, Op, 256, S>(p, axis, op); return; } break;
+            case 512: if constexpr (512 % T == 0 && DEF != 512) { launch_reg_th<Real, N, CONTIG, MODE, Op, 512, S>(p, axis, op); return; } break;
             default: break;
         }
     }
-    launch_reg_th<Real, N, CONTIG, MODE, Op, 0>(p, axis, op);
+    launch_reg_th<Real, N, CONTIG, MODE, Op, 0, S>(p, axis, op);
+}
+
+// Radix schedule: the plan's choice for the strided passes and for the stage boundary (the
+// other x passes keep schedule 0).
+template <typename Real, int N, bool CONTIG, int MODE, class Op>
+void launch_reg(gp5cu_plan *p, int axis, const Op &op) {
+    if constexpr (!CONTIG || MODE == MODE_INV_TURN_FWD) {
+        const int s = MODE == MODE_INV_TURN_FWD ? p->radix_boundary : p->radix[axis][MODE];
+        if (s == 1) {
+            launch_reg_s<Real, N, CONTIG, MODE, Op, 1>(p, axis, op);
+            return;
+        }
+    }
+    launch_reg_s<Real, N, CONTIG, MODE, Op, 0>(p, axis, op);
 }
 
 template <typename Real, bool CONTIG, int MODE, class Op>
@@ -237,7 +252,7 @@ static void kinetic_passes(gp5cu_plan *p, const void *src, void *w, const SolveP
     launch_axis<Real, false, MODE_INV>(p, 1, cp);
 }
 
-template <typename Real> void Launch<Real>::autotune(gp5cu_plan *p, int nrep) {
+template <typename Real> void Launch<Real>::autotune(gp5cu_plan *p, int nrep, bool radix) {
     using V = cpx<Real>;
     V *w = (V *)p->work;
     check_cuda(cudaMemsetAsync(w, 0, p->field_bytes * p->nsolve, p->stream), "memset work");
@@ -254,29 +269,71 @@ template <typename Real> void Launch<Real>::autotune(gp5cu_plan *p, int nrep) {
             default: launch_axis<Real, false, MODE_FWD_MID_INV>(p, axis, kin); break;
         }
     };
+    auto timed = [&](auto &&fn) {
+        fn();  // configure and warm
+        check_cuda(cudaEventRecord(e0, p->stream), "cudaEventRecord");
+        for (int r = 0; r < nrep; r++) fn();
+        check_cuda(cudaEventRecord(e1, p->stream), "cudaEventRecord");
+        check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+        return ms;
+    };
     try {
         for (int q = 0; q < kTunedPasses; q++) {
             const int axis = kTunedAxis[q], mode = kTunedMode[q];
             p->tile_threads[axis][mode] = 0;
             if (!p->ax[axis].reg) continue;  // the shared-memory engine has one tile shape
             float best = 0.f;
-            int best_th = 0;
-            for (int th : {128, 256, 512}) {
-                if (th % p->ax[axis].reg_threads != 0) continue;
-                p->tile_threads[axis][mode] = th;
-                run(q);  // configure and warm
-                check_cuda(cudaEventRecord(e0, p->stream), "cudaEventRecord");
-                for (int r = 0; r < nrep; r++) run(q);
-                check_cuda(cudaEventRecord(e1, p->stream), "cudaEventRecord");
-                check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
-                float ms = 0.f;
-                check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-                if (best_th == 0 || ms < best) {
-                    best = ms;
-                    best_th = th;
+            int best_th = 0, best_s = p->radix[axis][mode];
+            for (int s = 0; s < 2; s++) {
+                if (!radix && s != p->radix[axis][mode]) continue;
+                const int T = s == 0 ? p->ax[axis].reg_threads : p->ax[axis].reg_threads1;
+                for (int th : {128, 256, 512}) {
+                    if (th % T != 0) continue;
+                    p->radix[axis][mode] = s;
+                    p->tile_threads[axis][mode] = th;
+                    const float ms = timed([&] { run(q); });
+                    if (best_th == 0 || ms < best) {
+                        best = ms;
+                        best_th = th;
+                        best_s = s;
+                    }
                 }
             }
+            p->radix[axis][mode] = best_s;
             p->tile_threads[axis][mode] = best_th;
+        }
+        if (radix && p->ax[0].reg) {
+            // the stage boundary's schedule, timed on the work field alone (every operand of the
+            // RK stage epilogue points at it; each element is read and written by one thread)
+            EpiParams<Real> P{};
+            P.nsites = p->nsites;
+            P.mode = EPI_RK3;
+            P.psi = w;
+            P.psi_out = w;
+            P.kprev = w;
+            P.kout = w;
+            P.kacc = w;
+            P.ds = p->ds;
+            P.sp = p->sp_lap;
+            P.fkind = FK_LHY;
+            P.nx = p->shape[0];
+            P.ny = p->shape[1];
+            P.nz = p->shape[2];
+            P.slot = 1;
+            P.cfac = 0.5;
+            P.cnfac = 1.0;
+            P.turn = 1;
+            P.stream_aux = p->stream_aux ? 1 : 0;
+            OpStageOut<Real, false, true> op{w, P};
+            float ms[2];
+            for (int s = 0; s < 2; s++) {
+                p->radix_boundary = s;
+                ms[s] = timed([&] { launch_axis<Real, true, MODE_INV_TURN_FWD>(p, 0, op); });
+            }
+            p->radix_boundary = ms[1] < ms[0] ? 1 : 0;
+            check_cuda(cudaMemsetAsync(w, 0, p->field_bytes * p->nsolve, p->stream), "memset work");
         }
     } catch (...) {
         cudaEventDestroy(e0);

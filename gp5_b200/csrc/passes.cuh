@@ -214,9 +214,10 @@ template <class Op> struct has_mid_z<Op, std::void_t<decltype(Op::MID_Z)>> : std
 #ifndef GP5_HEAVY_THREADS
 #define GP5_HEAVY_THREADS 128
 #endif
-// TH > 0 overrides the rule (the autotuner's tile shapes for the strided y/z passes).
-template <typename Real, int N, bool CONTIG, int MODE, int TH = 0> struct RegTile {
-    static constexpr int T = RegCfgAll<N>::T;
+// TH > 0 overrides the rule (the autotuner's tile shapes for the strided y/z passes); S is the
+// radix schedule (RegCfg).
+template <typename Real, int N, bool CONTIG, int MODE, int TH = 0, int S = 0> struct RegTile {
+    static constexpr int T = RegCfgAll<N, S>::T;
     static constexpr int THREADS =
         TH > 0 ? TH
                : ((MODE == MODE_FWD_MID_INV || MODE == MODE_INV_TURN_FWD) && GP5_HEAVY_THREADS / T >= 2 ? GP5_HEAVY_THREADS
@@ -240,19 +241,31 @@ template <typename Real, int N, bool CONTIG, int MODE, int TH = 0> struct RegTil
 #ifndef GP5_C128_CAP
 #define GP5_C128_CAP 128
 #endif
-    static constexpr int REGCAP = sizeof(Real) == 8 ? GP5_C128_CAP
-                                                    : (STRIDED_COPY ? GP5_C64_CAP_COPY
-                                                                    : (MODE == MODE_INV_TURN_FWD ? GP5_C64_CAP_BOUNDARY
-                                                                                                 : GP5_C64_CAP_OTHER));
+#ifndef GP5_C128_CAP_LIGHT
+#define GP5_C128_CAP_LIGHT 96
+#endif
+#ifndef GP5_C64_CAP_LIGHT
+#define GP5_C64_CAP_LIGHT 64
+#endif
+    // a schedule with fewer elements per thread than S = 0 needs fewer registers: it is capped
+    // lower so that more CTAs share an SM
+    static constexpr bool LIGHT = RegCfg<N, S>::E < RegCfg<N, 0>::E;
+    static constexpr int REGCAP = LIGHT ? (sizeof(Real) == 8 ? GP5_C128_CAP_LIGHT : GP5_C64_CAP_LIGHT)
+                                        : (sizeof(Real) == 8 ? GP5_C128_CAP
+                                                             : (STRIDED_COPY ? GP5_C64_CAP_COPY
+                                                                             : (MODE == MODE_INV_TURN_FWD
+                                                                                    ? GP5_C64_CAP_BOUNDARY
+                                                                                    : GP5_C64_CAP_OTHER)));
     static constexpr int MINB_RAW = (65536 / REGCAP) / THREADS;
     static constexpr int MINB = MINB_RAW > 0 ? MINB_RAW : 1;
 };
 
-template <typename Real, int N, bool CONTIG, int MODE, class Op, int TH = 0>
-__global__ void __launch_bounds__(RegTile<Real, N, CONTIG, MODE, TH>::THREADS, RegTile<Real, N, CONTIG, MODE, TH>::MINB)
+template <typename Real, int N, bool CONTIG, int MODE, class Op, int TH = 0, int S = 0>
+__global__ void __launch_bounds__(RegTile<Real, N, CONTIG, MODE, TH, S>::THREADS,
+                                  RegTile<Real, N, CONTIG, MODE, TH, S>::MINB)
 k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedSlot rs) {
     using V = cpx<Real>;
-    constexpr int E = RegCfg<N>::E, T = RegCfgAll<N>::T, LINES = RegTile<Real, N, CONTIG, MODE, TH>::LINES;
+    constexpr int E = RegCfg<N, S>::E, T = RegCfgAll<N, S>::T, LINES = RegTile<Real, N, CONTIG, MODE, TH, S>::LINES;
     constexpr int NB = Op::BATCH;
     static_assert(E % NB == 0, "batch must divide the elements per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -299,8 +312,8 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
         }
         if constexpr (MODE == MODE_INV_TURN_FWD) {
             static_assert(CONTIG, "the stage boundary runs on x lines");
-            LayContig<N> lay;
-            reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+            LayContig<N, S> lay;
+            reg_fft<N, S, 1>(v, tid, line, tw, sm, lay);
             // The epilogue/prologue runs as a rolled loop over the thread's own elements staged
             // in shared memory: one copy of its code (the unrolled form overflowed the
             // instruction cache) and the transform registers are free meanwhile.  Each thread
@@ -326,11 +339,11 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
 #pragma unroll
             for (int m = 0; m < E; m++) v[m] = sm[lay(line, tid + T * m)];
             __syncthreads();
-            reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+            reg_fft<N, S, -1>(v, tid, line, tw, sm, lay);
         } else if constexpr (CONTIG) {
-            LayContig<N> lay;
-            if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
-            else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+            LayContig<N, S> lay;
+            if (MODE == MODE_INV) reg_fft<N, S, 1>(v, tid, line, tw, sm, lay);
+            else reg_fft<N, S, -1>(v, tid, line, tw, sm, lay);
             if (MODE == MODE_FWD_MID_INV) {
 #pragma unroll
                 for (int m = 0; m < E; m++) {
@@ -339,12 +352,12 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                     v[m] = op.mid(v[m], e, X);
                 }
                 __syncthreads();  // also a scheduling fence: keeps register pressure below 128
-                reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+                reg_fft<N, S, 1>(v, tid, line, tw, sm, lay);
             }
         } else {
             LayStrided lay{LINES};
-            if (MODE == MODE_INV) reg_fft<N, 1>(v, tid, line, tw, sm, lay);
-            else reg_fft<N, -1>(v, tid, line, tw, sm, lay);
+            if (MODE == MODE_INV) reg_fft<N, S, 1>(v, tid, line, tw, sm, lay);
+            else reg_fft<N, S, -1>(v, tid, line, tw, sm, lay);
             if constexpr (MODE == MODE_FWD_MID_INV && has_mid_z<Op>::value) {
                 if (g.axis == 2) {
                     // element m sits at tid + T*m < N/2 exactly when m < E/2, so the sign of
@@ -364,7 +377,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                     }
                 }
                 __syncthreads();  // also a scheduling fence: keeps register pressure below 128
-                reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+                reg_fft<N, S, 1>(v, tid, line, tw, sm, lay);
             } else if (MODE == MODE_FWD_MID_INV) {
 #pragma unroll
                 for (int m = 0; m < E; m++) {
@@ -373,7 +386,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                     v[m] = op.mid(v[m], e, X);
                 }
                 __syncthreads();  // also a scheduling fence: keeps register pressure below 128
-                reg_fft<N, 1>(v, tid, line, tw, sm, lay);
+                reg_fft<N, S, 1>(v, tid, line, tw, sm, lay);
             }
         }
         if (lr.valid && MODE == MODE_INV_TURN_FWD) {

@@ -24,7 +24,8 @@ struct ProfRec {
 struct AxisPlan {
     int n = 0;
     bool reg = false;     // register engine (power of two in [32, 512])
-    int reg_threads = 0;  // register engine: threads per line
+    int reg_threads = 0;  // register engine: threads per line (radix schedule 0)
+    int reg_threads1 = 0; // the same for radix schedule 1
     LineSchedule sched{};  // mixed-radix schedule for the shared-memory engine
     void *tw = nullptr;    // device twiddle table, plan precision, forward sign
     int smem_lines = 0;    // lines per tile of the shared-memory engine
@@ -82,6 +83,11 @@ struct gp5cu_plan {
     // threads per CTA of the register-engine passes along y/z, by [axis][mode] (0: the
     // default rule); chosen by the autotuner when the plan is created
     int tile_threads[3][4] = {};
+    // radix schedule (0 or 1, RegCfg) of the register-engine passes along y/z by [axis][mode],
+    // and of the stage boundary; chosen by the autotuner, the same for every plan of one
+    // (device, grid, components, precision)
+    int radix[3][4] = {};
+    int radix_boundary = 0;
     // launches of the stepper path use programmatic dependent launch (GP5_PDL=0 turns it off)
     bool pdl = true;
     // the stage boundary takes its tiles in reverse order (GP5_L2ORDER): it then starts on the
@@ -164,9 +170,10 @@ template <typename Real> struct Launch {
     static int step_merged(gp5cu_stepper *st, void *field, bool prologue);
     static void prologue(gp5cu_stepper *st, void *field);  // forward x transform of psi
     static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
-    // times every tile shape of the strided y/z passes on the zeroed work field and keeps
-    // the fastest in p->tile_threads
-    static void autotune(gp5cu_plan *p, int nrep);
+    // times every tile shape (and, with radix, both radix schedules) of the strided y/z passes
+    // on the zeroed work field, and with radix both schedules of the stage boundary; keeps the
+    // fastest in p->tile_threads, p->radix and p->radix_boundary
+    static void autotune(gp5cu_plan *p, int nrep, bool radix);
 };
 
 void set_scalars(cudaStream_t s, DevScalars *ds, int n = 1);

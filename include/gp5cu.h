@@ -305,20 +305,29 @@ int gp5cu_gemm_bf16(const void *A, long long sam, long long sak, const void *B, 
 #define GP5_GEMM_WAIT_DEFAULT_NS 2000000000ULL
 int gp5cu_mlp_set_wait_bound(gp5cu_mlp *net, unsigned long long ns);
 
-/* ---- tile-shape autotuner ----------------------------------------------------------------
+/* ---- tile-shape and radix autotuner -------------------------------------------------------
  * No reference counterpart (FFTW plans its own transforms).  The strided y/z passes of the
  * register engine (axis lengths 32..512, powers of two) come in tile shapes of 128, 256 or 512
- * threads per CTA (more threads = more consecutive x values per tile = wider coalesced rows).
- * gp5cu_plan_create times every shape of the five passes below on the plan's zeroed work field
- * and keeps the fastest; the choice is remembered per (device, shape, components, precision,
- * solves) for the life of the process.  GP5_AUTOTUNE=0 in the environment keeps the default
- * shapes.  These passes carry no reductions, so the tile shape changes no result bit.
+ * threads per CTA (more threads = more consecutive x values per tile = wider coalesced rows),
+ * and every register-engine pass along y/z, and the stage boundary along x, in two radix
+ * schedules (0: e.g. radix 16 x 16 at 256 with 16 elements per thread; 1: e.g. 8 x 8 x 4 with 8
+ * elements per thread, fewer registers, more resident CTAs).  gp5cu_plan_create times both
+ * schedules and every shape of the five passes below, and both schedules of the boundary, on
+ * the plan's zeroed work field and keeps the fastest.  The schedules round differently (at the
+ * level of the last bit), so they are chosen once per (device, grid, components, precision)
+ * and every later plan of that grid uses them whatever its number of solves; the thread
+ * counts change no result bit and are tuned per number of solves.  Choices are remembered for
+ * the life of the process and in a JSON file (GP5_AUTOTUNE_CACHE).  GP5_AUTOTUNE=0 keeps the
+ * default shapes and schedule 0; GP5_RADIX=0|1 fixes the schedules.
  * threads[5]: y forward, y inverse, z forward, z inverse, z forward*K^2*inverse; 0 = the
- * default shape (or an axis that uses the shared-memory engine).  Steppers capture the shapes
- * in their CUDA graphs when they first advance: set shapes before creating steppers. */
+ * default shape (or an axis that uses the shared-memory engine).  radix[6]: the schedules of
+ * the same five passes, then of the stage boundary.  Steppers capture both in their CUDA graphs
+ * when they first advance: set them before creating steppers. */
 int gp5cu_plan_autotune(gp5cu_plan *plan);
 int gp5cu_plan_get_tiles(const gp5cu_plan *plan, int threads[5]);
 int gp5cu_plan_set_tiles(gp5cu_plan *plan, const int threads[5]);
+int gp5cu_plan_get_radix(const gp5cu_plan *plan, int radix[6]);
+int gp5cu_plan_set_radix(gp5cu_plan *plan, const int radix[6]);
 
 /* ---- HDF5 field files ----------------------------------------------------------------------
  * The reference's on-disk format, read and written without libhdf5 (host only, no GPU):

@@ -90,3 +90,67 @@ def test_tuning_cache_file_is_written_and_reused(tmp_path):
     r2 = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
     assert r2.returncode == 0, r2.stderr
     assert eval(r2.stdout.strip().splitlines()[-1]) == [512, 256, 512, 256, 256]
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("shape", [(64, 32, 128), (256, 64, 64), (32, 512, 32), (128, 128, 256)])
+def test_both_radix_schedules_match_the_oracle(prec, shape):
+    """Schedules 0 and 1 (other radices, other elements per thread) each give the unnormalised
+    DFT and the spectral Laplacian to rounding: 1e-13 (complex128) / 2e-6 (complex64) of the
+    long-double-checked numpy transform and of the oracle."""
+    from gp5_b200 import _abi
+    from oracle import gp_oracle as o
+    geo = o.Geometry(shape, (-4.0,) * 3, (4.0,) * 3)
+    psi = _field(shape, 3)
+    ref_fwd = np.fft.fftn(psi, axes=(0, 1, 2))
+    ref_lap = o.laplacian(psi, geo)
+    tol = 1e-13 if prec == 0 else 2e-6
+    for s in (0, 1):
+        p = _abi.Plan(shape, geo.left, geo.right, precision=prec)
+        p.set_radix([s] * 6)
+        assert p.radix() == [s] * 6
+        src, dst = p.field(psi), p.field()
+        p.fft(src, dst, _abi.GP5_FORWARD)
+        got = dst.download()
+        assert np.max(np.abs(got - ref_fwd)) <= tol * np.max(np.abs(ref_fwd)), s
+        p.laplacian(src, dst)
+        got = dst.download()
+        assert np.max(np.abs(got - ref_lap)) <= tol * np.max(np.abs(ref_lap)), s
+
+
+@pytest.mark.parametrize("n", [32, 64, 128, 256])
+def test_radix_one_stage_boundary_rk4_step_matches_the_oracle(n):
+    """One renormalised imaginary-time RK4 step and one real-time step with every pass, the
+    stage boundary included, on schedule 1, against the oracle at 1e-12."""
+    from gp5_b200 import _abi
+    from oracle import gp_oracle as o
+    L = 4 * 100.0 ** (1 / 3)
+    geo = o.Geometry((n, n, n), (-L / 2,) * 3, (L / 2,) * 3)
+    psi = o.gaussian_with_noise(geo, 0.5 * 100.0 ** (1 / 3), 1e-3, seed=n, N=100.0, phase_noise=True)
+    for imag in (True, False):
+        p = _abi.Plan(geo.shape, geo.left, geo.right)
+        p.set_radix([1] * 6)
+        f = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=-3.1)
+        st = _abi.Stepper(f, 0.15 * (L / n) ** 2 if imag else 1e-3, imaginary=imag)
+        ost = o.Stepper(o.Functional("lhy", c3=-3.1), geo, st.dt, "RK4", imag)
+        if imag:
+            st.set_renormalization([100.0])
+            ost.normalizations = [100.0]
+        a = p.field(psi)
+        st.advance(a, 1)
+        ref = ost.advance(psi.copy(), 1)
+        got = a.download()
+        assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref)), imag
+
+
+def test_plans_of_one_grid_share_their_radix_schedules():
+    """The schedules are chosen once per grid and precision: a forced re-tune and a later plan
+    keep them (so batched and single solves round alike)."""
+    from gp5_b200 import _abi
+    a = _abi.Plan((64, 64, 32), (-1.0,) * 3, (1.0,) * 3)
+    r = a.radix()
+    a.autotune()
+    b = _abi.Plan((64, 64, 32), (-2.0,) * 3, (2.0,) * 3)
+    assert a.radix() == r and b.radix() == r
+    with pytest.raises(_abi.Gp5Error):
+        a.set_radix([2, 0, 0, 0, 0, 0])
