@@ -44,3 +44,18 @@ def test_roofline_traffic_comes_from_the_matching_precision():
 
 def test_unknown_profiles_give_no_roofline():
     assert bench.roofline({"profile": [(3, 1.0)] * 7, "field_bytes": 16}) is None
+
+
+def test_roofline_of_a_step_with_l2_slabs():
+    """With the y/z passes on x-slabs that stay in L2, only the slab's y forward read and its y
+    inverse write reach HBM: per stage 2F for the y/z work, 31F per step."""
+    F = 256 ** 3 * 16
+    prof = []
+    for s in range(4):
+        for _ in range(4):
+            prof += [(10, 0.02), (22, 0.03), (11, 0.02)]
+        prof.append((3, 0.3))
+    rf = bench.roofline({"profile": prof, "field_bytes": F}, "c128")
+    assert rf["kernel"] == "x_stage_boundary"
+    assert rf["step"]["algorithmic_bytes"] == pytest.approx(31 * F)
+    assert rf["per_kind_ms"]["z_fwd_kinetic_inv"] == pytest.approx(16 * 0.03)
