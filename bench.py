@@ -664,8 +664,11 @@ def main():
     results, launches = run_ours(args, rank, world, local_rank)
     gs = None
     if args.batch > 0:
-        gs = run_batch(args.batch, local_rank, rank=rank, world=world, precision="c128")
-        gs["c64"] = run_batch(args.batch, local_rank, rank=rank, world=world, precision="c64")
+        # the configuration's solves are shared out over the ranks (each draws its own seeded
+        # shard), so a run on N GPUs solves about the same number of droplets as one on 1 GPU
+        per_rank = max(1, args.batch // world)
+        gs = run_batch(per_rank, local_rank, rank=rank, world=world, precision="c128")
+        gs["c64"] = run_batch(per_rank, local_rank, rank=rank, world=world, precision="c64")
     prep = None
     if args.precision_report and world == 1:
         prep = precision_report(local_rank)

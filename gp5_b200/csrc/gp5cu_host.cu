@@ -406,10 +406,13 @@ gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const do
         {
             const char *pdl = std::getenv("GP5_PDL");
             p->pdl = !(pdl && std::string(pdl) == "0");
+            // defaults from the 256^3 step on a B200: the reversed boundary order saves 2% in
+            // both precisions; the evict-first hints save another 2% in complex64 and cost 1%
+            // in complex128
             const char *l2o = std::getenv("GP5_L2ORDER");
-            p->l2_order = l2o && std::string(l2o) == "1";
+            p->l2_order = l2o ? std::string(l2o) == "1" : true;
             const char *sa = std::getenv("GP5_STREAM_AUX");
-            p->stream_aux = sa && std::string(sa) == "1";
+            p->stream_aux = sa ? std::string(sa) == "1" : precision == GP5_C64;
             const char *yz = std::getenv("GP5_YZ_SLABS");
             if (yz) {
                 const int v = std::atoi(yz);

@@ -92,10 +92,11 @@ struct gp5cu_plan {
     bool pdl = true;
     // the stage boundary takes its tiles in reverse order (GP5_L2ORDER): it then starts on the
     // planes the y inverse pass wrote last, which are still in L2, and the next y forward pass
-    // starts on the planes the boundary wrote last
-    bool l2_order = false;
+    // starts on the planes the boundary wrote last (default on)
+    bool l2_order = true;
     // the stage boundary reads and writes psi and the k buffers with evict-first cache hints
-    // (GP5_STREAM_AUX), so that they do not push the transform buffer out of L2
+    // (GP5_STREAM_AUX), so that they do not push the transform buffer out of L2 (default: on
+    // for complex64 plans)
     bool stream_aux = false;
     // the merged RK step runs its y/z passes on this many slabs of consecutive x values
     // (GP5_YZ_SLABS; 1: one launch per pass over the whole field)

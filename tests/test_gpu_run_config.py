@@ -21,8 +21,9 @@ def test_trapped_gp_imaginary_rk4(tmp_path):
     np.save(tmp_path / "init.npy", psi)
     r = R.run(c, base=str(tmp_path), log=lambda *_: None)
     assert len(r["files"]) == 2 and r["steps"] == 20
-    out1 = np.load(r["files"][1])
-    assert np.array_equal(np.load(r["files"][0]), psi)
+    assert all(f.endswith(".hdf5") for f in r["files"])  # out_<k>.hdf5, as the reference writes
+    out1 = R.read_array(r["files"][1])
+    assert np.array_equal(R.read_array(r["files"][0]), psi)
     V = o.harmonic_potential(geo, [(1.0, 0.8, 1.2)])
     f = o.Functional("gp", couplings=np.array([[0.7]]), masses=[1.0], V=V)
     ref = o.Stepper(f, geo, 1e-3, "RK4", True, normalizations=[50.0]).advance(psi.copy(), 10)
@@ -57,4 +58,4 @@ def test_unlocked_droplet_with_file_potential_and_phase(tmp_path):
     V = Vf + (0.5 / (X * X + Y * Y))[..., None]
     f = o.Functional("lhy_unlocked", alpha=0.88, beta=1.0, eta=-4.0, V=V)
     ref = o.Stepper(f, geo, 5e-4, "eulero", False, constraint_phase=phase).advance(psi.copy(), 10)
-    assert rel(np.load(r["files"][1]), ref) < 1e-12
+    assert rel(R.read_array(r["files"][1]), ref) < 1e-12
