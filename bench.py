@@ -610,6 +610,39 @@ def cpu_reference_timing(max_seconds: float, max_steps: int, warmup: int = 1):
                       f"{o._WORKERS} workers, element-wise numpy over {o._WORKERS} threads"}
 
 
+def profiling_case(what: str) -> None:
+    """Small cases for ncu captures of single kernels (fields of 134-268 MB, above L2; about
+    1 GB on the device): step64 / step128 advance the bench workload two RK4 steps in
+    complex64 / complex128, obs128 evaluates the observables and the norm twice (the
+    point-wise reductions), cluster labels the droplets of the start state twice."""
+    import numpy as np
+
+    from gp5_b200 import _abi
+
+    shape, left, right = workload_geometry()
+    psi0 = initial_state()
+    if what in ("step64", "step128"):
+        prec = _abi.GP5_C64 if what == "step64" else _abi.GP5_C128
+        p = _abi.Plan(shape, left, right, precision=prec)
+        f = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
+        st = _abi.Stepper(f, DT, _abi.GP5_STEP_RK4, imaginary=False)
+        a = p.field(psi0)
+        st.advance(a, 2)
+        print("radix", p.radix(), "tiles", p.tiles(), "launches per step", st.launches_per_step)
+    elif what == "obs128":
+        p = _abi.Plan(shape, left, right)
+        f = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
+        a = p.field(psi0)
+        for _ in range(2):
+            print(f.observables(a), p.norm(a))
+    else:
+        p = _abi.Plan(shape, left, right)
+        a = p.field(psi0)
+        cut = 0.5 * float(np.max(np.abs(psi0)) ** 2)
+        for _ in range(2):
+            print("clusters", p.decompose(a, cut)[1])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -625,7 +658,12 @@ def main():
                     help="also run the complex64-vs-complex128 quench report and write it here")
     ap.add_argument("--batch", type=int, default=64,
                     help="solves of the ground-state leg, in complex128 and in complex64 (0: skip)")
+    ap.add_argument("--case", choices=["step64", "step128", "obs128", "cluster"],
+                    help="run one small profiling case of the workload and exit (no JSON line)")
     args = ap.parse_args()
+    if args.case:
+        profiling_case(args.case)
+        return
     if args.warmup < 3:
         args.warmup = 3
 
