@@ -23,6 +23,7 @@ GP5_OK, GP5_ERR_ARG, GP5_ERR_CUDA, GP5_ERR_NONFINITE, GP5_ERR_TIMEOUT = 0, 1, 2,
 GP5_ERR_UNSUPPORTED, GP5_ERR_STATE, GP5_ERR_NOMEM, GP5_ERR_IO = 5, 6, 7, 8
 GP5_C128, GP5_C64 = 0, 1
 GP5_GEMM_WAIT_DEFAULT_NS = 2_000_000_000
+GP5_RING_WAIT_DEFAULT_NS = 2_000_000_000
 GP5_FORWARD, GP5_BACKWARD = -1, 1
 GP5_FUNC_GP, GP5_FUNC_LHY, GP5_FUNC_LHY_UNLOCKED = 0, 1, 2
 GP5_POT_NONE, GP5_POT_HARMONIC, GP5_POT_ARRAY = 0, 1, 2
@@ -150,6 +151,7 @@ def lib():
         "gp5cu_plan_set_tiles": (i, [vp, C.POINTER(C.c_int)]),
         "gp5cu_plan_get_radix": (i, [vp, C.POINTER(C.c_int)]),
         "gp5cu_plan_set_radix": (i, [vp, C.POINTER(C.c_int)]),
+        "gp5cu_plan_set_wait_bound": (i, [vp, C.c_ulonglong]),
         "gp5cu_mlp_create": (i, [pp, i, C.c_ulonglong]),
         "gp5cu_mlp_destroy": (i, [vp]),
         "gp5cu_mlp_num_params": (C.c_longlong, [vp]),
@@ -253,7 +255,8 @@ class Plan:
         check(lib().gp5cu_plan_set_tiles(self.h, t))
 
     def radix(self):
-        """Radix schedules (0/1) of (y fwd, y inv, z fwd, z inv, z fwd*K^2*inv, x stage boundary)."""
+        """Radix schedules (0/1) of (y fwd, y inv, z fwd, z inv, z fwd*K^2*inv), then the x stage
+        boundary's choice (bit 0 schedule, bit 1 bulk-copy ring)."""
         r = (C.c_int * 6)()
         check(lib().gp5cu_plan_get_radix(self.h, r))
         return list(r)
@@ -261,6 +264,10 @@ class Plan:
     def set_radix(self, radix) -> None:
         r = (C.c_int * 6)(*[int(v) for v in radix])
         check(lib().gp5cu_plan_set_radix(self.h, r))
+
+    def set_wait_bound(self, ns: int) -> None:
+        """Bound of the bulk-copy ring's stage waits (gp5cu_plan_set_wait_bound)."""
+        check(lib().gp5cu_plan_set_wait_bound(self.h, int(ns)))
 
     def autotune(self) -> None:
         check(lib().gp5cu_plan_autotune(self.h))

@@ -27,7 +27,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--ex
 
 CU_SOURCES = ["gp5cu_f64.cu", "gp5cu_f32.cu", "gp5cu_host.cu", "gp5cu_batch.cu", "gp5cu_noalloc.cu", "mlp.cu",
               "gp5cu_cluster.cu", "gp5cu_h5.cpp"]
-HEADERS = ["common.cuh", "fft_line.cuh", "passes.cuh", "ops.cuh", "launch_impl.cuh", "plan.hpp"]
+HEADERS = ["common.cuh", "fft_line.cuh", "passes.cuh", "ops.cuh", "ring.cuh", "launch_impl.cuh", "plan.hpp"]
 
 
 def _newer(target: str, deps) -> bool:

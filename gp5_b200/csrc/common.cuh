@@ -26,6 +26,41 @@ template <typename V> __host__ __device__ __forceinline__ V cadd(V a, V b) {
 template <typename V> __host__ __device__ __forceinline__ V csub(V a, V b) {
     V r; r.x = a.x - b.x; r.y = a.y - b.y; return r;
 }
+// complex64 sums and differences as one packed two-lane FP32 instruction (add/sub.rn.f32x2 of
+// sm_100a, each lane rounded as the scalar operation is).  Default on: the complex64 step is
+// issue-bound and measured 4.6% faster at 256^3 (every pass gained).  The packed forms are not
+// contracted with a neighbouring multiply, so results differ from GP5_F32X2=0 in the last bits.
+#ifndef GP5_F32X2
+#define GP5_F32X2 1
+#endif
+#if GP5_F32X2
+template <> __host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+    unsigned long long x, y, d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(y) : "f"(b.x), "f"(b.y));
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(x), "l"(y));
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(d));
+    return r;
+#else
+    return float2{a.x + b.x, a.y + b.y};
+#endif
+}
+template <> __host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+    unsigned long long x, y, d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(y) : "f"(b.x), "f"(b.y));
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(x), "l"(y));
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(d));
+    return r;
+#else
+    return float2{a.x - b.x, a.y - b.y};
+#endif
+}
+#endif
 // (a+ib)(c+id) = (ac - bd) + i(ad + bc), the order std::complex uses
 template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
     V r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;

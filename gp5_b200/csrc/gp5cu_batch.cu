@@ -35,6 +35,7 @@ struct BatchGroup {
     gp5cu_stepper *st = nullptr;
     void *psi = nullptr;  // idx.size() consecutive fields
     std::vector<DevScalars> ds_host;
+    std::vector<DevScalars> st_host;  // the stepper's scalars (status of the bounded waits)
 };
 
 struct gp5cu_batch {
@@ -134,6 +135,7 @@ void make_group(BatchGroup &g, const std::vector<gp5cu_solve_desc> &solves, int 
     check_cuda(cudaMalloc(&g.psi, g.plan->field_bytes * k), "cudaMalloc batch states");
     check_cuda(cudaMemset(g.psi, 0, g.plan->field_bytes * k), "memset batch states");
     g.ds_host.resize(k);
+    g.st_host.resize(k);
     g.live = k;
 }
 
@@ -249,6 +251,9 @@ std::vector<int> run_phase(gp5cu_batch *b, int set, int check_every, const std::
                         check_cuda(cudaGraphLaunch(st->exec, p->stream), "cudaGraphLaunch");
                     Launch<Real>::scale(p, g.psi, -1, st->ds, true);  // pending normalisation
                     b->launches += 3 + (long long)check_every * st->launches_per_step;
+                    check_cuda(cudaMemcpyAsync(g.st_host.data(), st->ds, sizeof(DevScalars) * g.live,
+                                               cudaMemcpyDeviceToHost, p->stream),
+                               "read batch step status");
                 }
                 set_scalars(p->stream, p->ds, p->nsolve);
                 Launch<Real>::apply_h(g.func, g.psi, p->work, true);
@@ -269,6 +274,8 @@ std::vector<int> run_phase(gp5cu_batch *b, int set, int check_every, const std::
             int kept = 0;
             for (int q = 0; q < g.live; q++) {
                 const int i = g.idx[q];
+                if (check > 0 && (g.st_host[q].status & DS_TIMEOUT))
+                    fail(GP5_ERR_TIMEOUT, "a bounded device wait ran out (solve " + std::to_string(i) + ")");
                 if (check > 0) steps[i] += check_every;
                 const DevScalars &d = g.ds_host[q];
                 const double dV = g.plan->sp_host[q].dV;

@@ -216,7 +216,9 @@ static SolveParams geometry_params(const int shape[3], const double left[3], con
 // (empty: no file), default $XDG_CACHE_HOME/gp5_b200/autotune.json or
 // ~/.cache/gp5_b200/autotune.json.  Two kinds of entries:
 //   "radix|<device>|<nx>x<ny>x<nz>|c<ncomp>|<c128|c64>|build <date time>": the radix schedule
-//     (0/1) of the five tuned passes of gp5cu_plan_get_tiles and of the stage boundary.  The
+//     (0/1) of the five tuned passes of gp5cu_plan_get_tiles and of the stage boundary, whose
+//     entry also carries (bit 1) the bulk-copy ring feed: its tiles have other line counts, so
+//     its per-tile partial sums fold in another order.  The
 //     schedules round differently, so they are chosen once per grid and precision and every
 //     plan of that grid uses them, whatever its number of solves (a batch is then bitwise a
 //     set of single solves);
@@ -224,7 +226,8 @@ static SolveParams geometry_params(const int shape[3], const double left[3], con
 //     five thread counts of gp5cu_plan_get_tiles for those schedules (they change no result
 //     bit).
 // GP5_AUTOTUNE=0 keeps the default shapes and schedule 0; GP5_RADIX=0 or 1 fixes the schedule
-// of every tuned pass and of the boundary (the thread counts are still tuned).
+// of every tuned pass and of the boundary (the thread counts are still tuned); GP5_RING=0 or 1
+// then fixes the boundary's feed.
 static std::mutex g_tune_mu;
 static std::map<std::string, std::vector<int>> g_tune_cache;
 static bool g_tune_loaded = false;
@@ -273,7 +276,12 @@ static void tune_cache_load(const std::string &path) {
         }
         const bool is_radix = key.compare(0, 6, "radix|") == 0;
         bool ok = (int)v.size() == (is_radix ? kTunedPasses + 1 : kTunedPasses);
-        for (int x : v) ok = ok && (is_radix ? (x == 0 || x == 1) : (x == 0 || x == 128 || x == 256 || x == 512));
+        for (size_t q = 0; q < v.size(); q++) {
+            const int x = v[q];
+            // radix entries: 0/1 per tuned pass; the boundary's entry also carries the ring bit
+            const int hi = (is_radix && (int)q == kTunedPasses) ? 3 : 1;
+            ok = ok && (is_radix ? (x >= 0 && x <= hi) : (x == 0 || x == 128 || x == 256 || x == 512));
+        }
         if (ok) g_tune_cache[key] = v;
         pos = close + 1;
     }
@@ -349,6 +357,8 @@ void autotune_plan(gp5cu_plan *p, bool force) {
     const char *fixed = std::getenv("GP5_RADIX");
     if (fixed && (std::string(fixed) == "0" || std::string(fixed) == "1")) {
         apply_radix(p, std::vector<int>(kTunedPasses + 1, std::atoi(fixed)));
+        const char *ring = std::getenv("GP5_RING");
+        if (ring && std::string(ring) == "1" && p->ax[0].reg) p->radix_boundary |= 2;
         have_radix = true;
     } else {
         // a forced re-tune times the thread counts again but keeps the grid's schedules, so
@@ -558,7 +568,9 @@ int gp5cu_plan_get_radix(const gp5cu_plan *p, int radix[6]) {
 int gp5cu_plan_set_radix(gp5cu_plan *p, const int radix[6]) {
     GP5_TRY
     require(p != nullptr && radix != nullptr, "NULL argument");
-    for (int q = 0; q <= kTunedPasses; q++) require(radix[q] == 0 || radix[q] == 1, "radix schedules are 0 or 1");
+    for (int q = 0; q < kTunedPasses; q++) require(radix[q] == 0 || radix[q] == 1, "radix schedules are 0 or 1");
+    require(radix[kTunedPasses] >= 0 && radix[kTunedPasses] <= 3,
+            "the stage boundary's choice is 0-3 (bit 0 schedule, bit 1 bulk-copy ring)");
     for (int q = 0; q < kTunedPasses; q++) {
         const int axis = kTunedAxis[q], mode = kTunedMode[q];
         const AxisPlan &ap = p->ax[axis];
@@ -569,6 +581,13 @@ int gp5cu_plan_set_radix(gp5cu_plan *p, const int radix[6]) {
             p->tile_threads[axis][mode] = 0;
     }
     p->radix_boundary = p->ax[0].reg ? radix[kTunedPasses] : 0;
+    GP5_CATCH
+}
+
+int gp5cu_plan_set_wait_bound(gp5cu_plan *p, unsigned long long ns) {
+    GP5_TRY
+    require(p != nullptr, "plan is NULL");
+    p->ring_wait_ns = ns;
     GP5_CATCH
 }
 

@@ -9,6 +9,7 @@
 
 #include "ops.cuh"
 #include "plan.hpp"
+#include "ring.cuh"
 
 namespace gp5 {
 
@@ -120,12 +121,43 @@ void launch_reg_s(gp5cu_plan *p, int axis, const Op &op) {
     launch_reg_th<Real, N, CONTIG, MODE, Op, 0, S>(p, axis, op);
 }
 
+// The stage boundary on the bulk-copy ring (ring.cuh): one persistent CTA per SM (its shared
+// memory holds the ring).  Returns false when the ring does not serve this configuration
+// (tile shape, or the compensated complex64 update, whose BF16 stream is not staged).
+template <typename Real, int N, int S, class Op> bool launch_ring(gp5cu_plan *, const Op &) { return false; }
+template <typename Real, int N, int S, bool RED>
+bool launch_ring(gp5cu_plan *p, const OpStageOut<Real, RED, true> &op) {
+    using RT = RingTile<Real, N, S>;
+    if constexpr (!RT::OK) {
+        return false;
+    } else {
+        if (op.P.comp) return false;
+        long long tiles = 0;
+        TileGeom g = make_geom(p, 0, RT::LINES, true, &tiles);
+        g.reverse = p->l2_order ? 1 : 0;
+        auto kern = k_boundary_ring<Real, N, S, RED>;
+        ensure_smem(kern, RT::SMEM, p->dev);
+        if (p->dry) return true;
+        const unsigned grid = (unsigned)std::min<long long>(tiles, p->sms);
+        launch_k(p, kern, grid, RT::THREADS, RT::SMEM, g, op, (const cpx<Real> *)p->ax[0].tw, red_slot(p),
+                 p->ring_wait_ns);
+        if (p->prof) p->prof->record(p->stream, MODE_INV_TURN_FWD);
+        return true;
+    }
+}
+
 // Radix schedule: the plan's choice for the strided passes and for the stage boundary (the
-// other x passes keep schedule 0).
+// other x passes keep schedule 0).  The boundary's choice also selects its operand feed: bit 0
+// the schedule, bit 1 the bulk-copy ring instead of register loads.
 template <typename Real, int N, bool CONTIG, int MODE, class Op>
 void launch_reg(gp5cu_plan *p, int axis, const Op &op) {
+    if constexpr (MODE == MODE_INV_TURN_FWD) {
+        if (p->radix_boundary & 2) {
+            if ((p->radix_boundary & 1) ? launch_ring<Real, N, 1>(p, op) : launch_ring<Real, N, 0>(p, op)) return;
+        }
+    }
     if constexpr (!CONTIG || MODE == MODE_INV_TURN_FWD) {
-        const int s = MODE == MODE_INV_TURN_FWD ? p->radix_boundary : p->radix[axis][MODE];
+        const int s = MODE == MODE_INV_TURN_FWD ? (p->radix_boundary & 1) : p->radix[axis][MODE];
         if (s == 1) {
             launch_reg_s<Real, N, CONTIG, MODE, Op, 1>(p, axis, op);
             return;
@@ -252,6 +284,19 @@ static void kinetic_passes(gp5cu_plan *p, const void *src, void *w, const SolveP
     launch_axis<Real, false, MODE_INV>(p, 1, cp);
 }
 
+// whether the ring kernel has a tile shape for the plan's x length and schedule s
+template <typename Real> bool ring_serves(const gp5cu_plan *p, int s) {
+    if (!p->ax[0].reg) return false;
+    switch (p->shape[0]) {
+        case 32: return s ? RingTile<Real, 32, 1>::OK : RingTile<Real, 32, 0>::OK;
+        case 64: return s ? RingTile<Real, 64, 1>::OK : RingTile<Real, 64, 0>::OK;
+        case 128: return s ? RingTile<Real, 128, 1>::OK : RingTile<Real, 128, 0>::OK;
+        case 256: return s ? RingTile<Real, 256, 1>::OK : RingTile<Real, 256, 0>::OK;
+        case 512: return s ? RingTile<Real, 512, 1>::OK : RingTile<Real, 512, 0>::OK;
+        default: return false;
+    }
+}
+
 template <typename Real> void Launch<Real>::autotune(gp5cu_plan *p, int nrep, bool radix) {
     using V = cpx<Real>;
     V *w = (V *)p->work;
@@ -327,12 +372,19 @@ template <typename Real> void Launch<Real>::autotune(gp5cu_plan *p, int nrep, bo
             P.turn = 1;
             P.stream_aux = p->stream_aux ? 1 : 0;
             OpStageOut<Real, false, true> op{w, P};
-            float ms[2];
-            for (int s = 0; s < 2; s++) {
-                p->radix_boundary = s;
-                ms[s] = timed([&] { launch_axis<Real, true, MODE_INV_TURN_FWD>(p, 0, op); });
+            // schedules 0 / 1 with register loads, then on the bulk-copy ring where it serves
+            float best = 0.f;
+            int best_b = 0;
+            for (int b = 0; b < 4; b++) {
+                if ((b & 2) && !ring_serves<Real>(p, b & 1)) continue;
+                p->radix_boundary = b;
+                const float ms = timed([&] { launch_axis<Real, true, MODE_INV_TURN_FWD>(p, 0, op); });
+                if (b == 0 || ms < best) {
+                    best = ms;
+                    best_b = b;
+                }
             }
-            p->radix_boundary = ms[1] < ms[0] ? 1 : 0;
+            p->radix_boundary = best_b;
             check_cuda(cudaMemsetAsync(w, 0, p->field_bytes * p->nsolve, p->stream), "memset work");
         }
     } catch (...) {

@@ -186,9 +186,16 @@ __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
 
 // L2 prefetch of every stream of a contiguous x tile that reads more than one array: one
 // instruction per stream, issued by thread 0 at kernel start, so that all DRAM reads of the
-// tile are in flight at once and the later register loads hit L2.
+// tile are in flight at once and the later register loads hit L2.  GP5_PREFETCH_AUX: 2 all
+// streams, 1 the epilogue's streams only (not the transform input), 0 none (default: with the
+// reversed boundary tile order the prefetch measured 1-2% slower at 256^3 in both precisions,
+// and its lines were partly evicted before use: 8-18% extra DRAM reads in stages 2-4).
+#ifndef GP5_PREFETCH_AUX
+#define GP5_PREFETCH_AUX 0
+#endif
 template <typename V, class Op>
 __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, const Op &op) {
+    if constexpr (GP5_PREFETCH_AUX == 0) return;
     const void *st[4];
     const int ns = op.streams(st);
     if (ns < 2 || threadIdx.x != 0 || g.axis != 0) return;
@@ -197,7 +204,7 @@ __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, 
     long long L1 = L0 + g.lines;
     if (L1 > g.n_other) L1 = g.n_other;
     const long long e0 = solve * g.solve_stride + L0 * g.nx, cnt = (L1 - L0) * g.nx;
-    for (int q = 0; q < ns; q++)
+    for (int q = GP5_PREFETCH_AUX == 1 ? 1 : 0; q < ns; q++)
         prefetch_l2(reinterpret_cast<const V *>(st[q]) + e0, (unsigned)(cnt * sizeof(V)));
 }
 

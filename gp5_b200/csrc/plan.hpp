@@ -103,6 +103,8 @@ struct gp5cu_plan {
     int yz_slabs = 1;
     // x range of the strided (y/z) launches being queued: [xr0, xr0 + xr_n), or all when 0
     int xr0 = 0, xr_n = 0;
+    // bound of the bulk-copy ring's waits (gp5cu_plan_set_wait_bound)
+    unsigned long long ring_wait_ns = GP5_RING_WAIT_DEFAULT_NS;
 };
 
 struct gp5cu_functional {

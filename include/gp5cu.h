@@ -321,13 +321,26 @@ int gp5cu_mlp_set_wait_bound(gp5cu_mlp *net, unsigned long long ns);
  * default shapes and schedule 0; GP5_RADIX=0|1 fixes the schedules.
  * threads[5]: y forward, y inverse, z forward, z inverse, z forward*K^2*inverse; 0 = the
  * default shape (or an axis that uses the shared-memory engine).  radix[6]: the schedules of
- * the same five passes, then of the stage boundary.  Steppers capture both in their CUDA graphs
- * when they first advance: set them before creating steppers. */
+ * the same five passes, then the stage boundary's choice: bit 0 its schedule, bit 1 its operand
+ * feed (0: register loads, one tile per CTA; 1: the bulk-copy ring, one persistent CTA per SM
+ * whose tiles' streams arrive by cp.async.bulk into a ring of shared-memory stages while the
+ * previous tile transforms; where the ring has no tile shape for the schedule, or for the
+ * compensated complex64 update, the register-load kernel runs).  The autotuner times all four
+ * boundary choices.  Steppers capture these choices in their CUDA graphs when they first
+ * advance: set them before creating steppers. */
 int gp5cu_plan_autotune(gp5cu_plan *plan);
 int gp5cu_plan_get_tiles(const gp5cu_plan *plan, int threads[5]);
 int gp5cu_plan_set_tiles(gp5cu_plan *plan, const int threads[5]);
 int gp5cu_plan_get_radix(const gp5cu_plan *plan, int radix[6]);
 int gp5cu_plan_set_radix(gp5cu_plan *plan, const int radix[6]);
+/* Bound of the bulk-copy ring's device-side wait for a stage's copies (default
+ * GP5_RING_WAIT_DEFAULT_NS = 2 s), for launches queued or captured afterwards.  When a wait
+ * runs out, the CTA stops taking tiles, waits (with the fixed 2 s bound) for the copies it
+ * issued and flags DS_TIMEOUT: the stepper call then returns GP5_ERR_TIMEOUT and the plan
+ * stays usable.  A bound of 0 fails every wait whose copies have not landed at the first probe
+ * (used to test the path). */
+#define GP5_RING_WAIT_DEFAULT_NS 2000000000ULL
+int gp5cu_plan_set_wait_bound(gp5cu_plan *plan, unsigned long long ns);
 
 /* ---- HDF5 field files ----------------------------------------------------------------------
  * The reference's on-disk format, read and written without libhdf5 (host only, no GPU):
