@@ -218,13 +218,18 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream(device=dev)
     results = {}
     launches = 0
-    for key, prec, comp in ((0, _abi.GP5_C128, False), (1, _abi.GP5_C64, False), (2, _abi.GP5_C64, True)):
+    # complex128; complex64 as created (stochastically rounded state update); complex64 with the
+    # compensated update; complex64 rounded to nearest
+    for key, prec, form in ((0, _abi.GP5_C128, ""), (1, _abi.GP5_C64, ""), (2, _abi.GP5_C64, "comp"),
+                            (3, _abi.GP5_C64, "rn")):
         plan = _abi.Plan(shape, left, right, precision=prec, device=dev)
         plan.set_stream(stream.cuda_stream)
         func = _abi.Functional(plan, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
         st = _abi.Stepper(func, DT, _abi.GP5_STEP_RK4, imaginary=False)
-        if comp:
+        if form == "comp":
             st.set_compensation(True)
+        elif form == "rn":
+            st.set_stochastic_rounding(False)
         f = plan.field(psi0)
         st.advance(f, args.warmup)  # builds the step graph; W untimed steps
         with torch.cuda.stream(stream):
@@ -344,8 +349,9 @@ def roofline(r, dtype: str = "c128"):
 def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float = 1e-8):
     """Ground state at c3 = -3 (imaginary-time RK4 to the residual tol, complex128), then the
     quench c3 -> -3.3 in real time for `steps` RK4 steps of dt = 5e-5 in complex128 and in
-    complex64 from the same state; every `every` steps the norm and the energy of both (FP64
-    reductions) and the complex64 energy error against complex128."""
+    complex64 from the same state (three complex64 forms: as created, with the stochastically
+    rounded state update; compensated; rounded to nearest); every `every` steps the norm and
+    the energy (FP64 reductions) and each complex64 form's energy error against complex128."""
     import numpy as np
     import torch
 
@@ -375,8 +381,8 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
     e_field = p64.field()
     p32 = None
     ms_adv = {}
-    for prec, name, comp in ((_abi.GP5_C128, "c128", False), (_abi.GP5_C64, "c64", False),
-                             (_abi.GP5_C64, "c64c", True)):
+    for prec, name, form in ((_abi.GP5_C128, "c128", ""), (_abi.GP5_C64, "c64", ""),
+                             (_abi.GP5_C64, "c64c", "comp"), (_abi.GP5_C64, "c64rn", "rn")):
         if prec == _abi.GP5_C128:
             p = p64
         else:
@@ -384,8 +390,10 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
             p = p32
         fq = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
         sq = _abi.Stepper(fq, DT, _abi.GP5_STEP_RK4, imaginary=False)
-        if comp:
+        if form == "comp":
             sq.set_compensation(True)
+        elif form == "rn":
+            sq.set_stochastic_rounding(False)
         g = p.field(psi0)
         out = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -410,19 +418,29 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
         del g, sq, fq
     table = []
     n0 = rows["c128"][0][1]
-    for (k, n64, e64, _), (_, n32, e32, e32s), (_, nc, ec, ecs) in zip(rows["c128"], rows["c64"], rows["c64c"]):
-        table.append({"step": k, "norm_c128": n64, "norm_c64": n32, "norm_c64c": nc, "energy_c128": e64,
-                      "energy_c64": e32, "energy_c64c": ec, "energy_c64_state_in_c128": e32s,
+    for (k, n64, e64, _), (_, n32, e32, e32s), (_, nc, ec, ecs), (_, nr, er, ers) in zip(
+            rows["c128"], rows["c64"], rows["c64c"], rows["c64rn"]):
+        table.append({"step": k, "norm_c128": n64, "norm_c64": n32, "norm_c64c": nc, "norm_c64rn": nr,
+                      "energy_c128": e64, "energy_c64": e32, "energy_c64c": ec, "energy_c64rn": er,
+                      "energy_c64_state_in_c128": e32s, "energy_c64c_state_in_c128": ecs,
+                      "energy_c64rn_state_in_c128": ers,
                       "norm_drift_c128": (n64 - n0) / n0, "norm_drift_c64": (n32 - n0) / n0,
-                      "norm_drift_c64c": (nc - n0) / n0,
+                      "norm_drift_c64c": (nc - n0) / n0, "norm_drift_c64rn": (nr - n0) / n0,
                       "energy_rel_err_c64": abs(e32 - e64) / abs(e64),
                       "energy_rel_err_c64_state": abs(e32s - e64) / abs(e64),
-                      "energy_rel_err_c64c": abs(ec - e64) / abs(e64)})
+                      "energy_rel_err_c64c": abs(ec - e64) / abs(e64),
+                      "energy_rel_err_c64c_state": abs(ecs - e64) / abs(e64),
+                      "energy_rel_err_c64rn": abs(er - e64) / abs(e64),
+                      "energy_rel_err_c64rn_state": abs(ers - e64) / abs(e64)})
     return {"ground_state": gs, "checkpoints": table, "ms_per_step_median": ms_adv,
             "max_energy_rel_err_c64c": max(r["energy_rel_err_c64c"] for r in table),
             "max_norm_drift_c64c": max(abs(r["norm_drift_c64c"]) for r in table),
             "max_energy_rel_err_c64": max(r["energy_rel_err_c64"] for r in table),
             "max_energy_rel_err_c64_state": max(r["energy_rel_err_c64_state"] for r in table),
+            "max_energy_rel_err_c64c_state": max(r["energy_rel_err_c64c_state"] for r in table),
+            "max_energy_rel_err_c64rn": max(r["energy_rel_err_c64rn"] for r in table),
+            "max_energy_rel_err_c64rn_state": max(r["energy_rel_err_c64rn_state"] for r in table),
+            "max_norm_drift_c64rn": max(abs(r["norm_drift_c64rn"]) for r in table),
             "max_norm_drift_c128": max(abs(r["norm_drift_c128"]) for r in table),
             "max_norm_drift_c64": max(abs(r["norm_drift_c64"]) for r in table),
             "workload": "N=5000 LHY droplet, 256^3, L=4 N^(1/3); ground state at c3=-3 (residual 1e-8), "
@@ -430,7 +448,8 @@ def precision_report(dev: int, steps: int = 5000, every: int = 500, tol: float =
 
 
 def precision_check(dev: int, steps: int = 500, every: int = 100):
-    """complex64 (plain and compensated) against complex128 on the bench workload itself: the
+    """complex64 (as created: stochastic state rounding; compensated; rounded to nearest) against
+    complex128 on the bench workload itself: the
     same initial state, `steps` real-time RK4 steps of the quenched droplet in each precision;
     every `every` steps the norm and the energy (FP64 reductions, complex64 state evaluated by
     the complex128 functional) against the complex128 run.  Returns the maxima."""
@@ -445,11 +464,13 @@ def precision_check(dev: int, steps: int = 500, every: int = 100):
     f_eval = _abi.Functional(p64, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
     e_field = p64.field()
     rows = {}
-    for name, p, comp in (("c128", p64, False), ("c64", p32, False), ("c64c", p32, True)):
+    for name, p, form in (("c128", p64, ""), ("c64", p32, ""), ("c64c", p32, "comp"), ("c64rn", p32, "rn")):
         fq = _abi.Functional(p, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
         sq = _abi.Stepper(fq, DT, _abi.GP5_STEP_RK4, imaginary=False)
-        if comp:
+        if form == "comp":
             sq.set_compensation(True)
+        elif form == "rn":
+            sq.set_stochastic_rounding(False)
         g = p.field(psi0)
         out = []
         for k in range(0, steps + 1, every):
@@ -467,7 +488,7 @@ def precision_check(dev: int, steps: int = 500, every: int = 100):
     n0 = ref[0][0]
     res = {"steps": steps, "every": every,
            "max_norm_drift_c128": max(abs(n - n0) / n0 for n, _ in ref)}
-    for name in ("c64", "c64c"):
+    for name in ("c64", "c64c", "c64rn"):
         res["max_energy_rel_err_" + name] = max(abs(e - er) / abs(er) for (_, e), (_, er) in zip(rows[name], ref))
         res["max_norm_drift_" + name] = max(abs(n - n0) / n0 for n, _ in rows[name])
     res["workload"] = ("bench workload (Gaussian start, c3=-3.3), real-time RK4 dt=5e-5 in each precision "
@@ -719,7 +740,7 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
-    r64, r32, r32c = results[0], results[1], results[2]
+    r64, r32, r32c, r32n = results[0], results[1], results[2], results[3]
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         c = cpu_reference_timing(max_seconds=20.0, max_steps=4, warmup=0)
@@ -734,8 +755,9 @@ def main():
             d.pop("_steps")
             d.pop("_grids")
     energy = ({k: prep[k] for k in ("max_energy_rel_err_c64", "max_energy_rel_err_c64_state", "max_energy_rel_err_c64c",
-                                    "max_norm_drift_c64c", "ms_per_step_median", "max_norm_drift_c64",
-                                    "max_norm_drift_c128")} if prep else
+                                    "max_energy_rel_err_c64c_state", "max_energy_rel_err_c64rn",
+                                    "max_energy_rel_err_c64rn_state", "max_norm_drift_c64c", "max_norm_drift_c64rn",
+                                    "ms_per_step_median", "max_norm_drift_c64", "max_norm_drift_c128")} if prep else
               (None if args.no_precision_check else precision_check(local_rank)))
     line = {"metric": metric, "value": r64["value"], "unit": "site-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r64["ms_per_step"],
@@ -745,10 +767,15 @@ def main():
                      "speedup_vs_fp64": r32["value"] / r64["value"], "clocks": r32["clocks"],
                      "roofline": roofline(dict(r32, field_bytes=r64["field_bytes"] // 2), "c64"),
                      "energy_error": energy,
+                     "state_rounding": "stochastic (the complex64 default, gp5cu_stepper_set_stochastic_rounding)",
                      "compensated": {"value": r32c["value"], "ms_per_step": r32c["ms_per_step"],
                                      "speedup_vs_fp64": r32c["value"] / r64["value"], "clocks": r32c["clocks"],
                                      "note": "gp5cu_stepper_set_compensation: BF16 correction field, "
-                                             "two-sum state update"}},
+                                             "two-sum state update"},
+                     "round_to_nearest": {"value": r32n["value"], "ms_per_step": r32n["ms_per_step"],
+                                          "speedup_vs_fp64": r32n["value"] / r64["value"],
+                                          "clocks": r32n["clocks"],
+                                          "note": "gp5cu_stepper_set_stochastic_rounding(0)"}},
             "e2e": r64["e2e"], "roofline": roofline(r64, "c128"), "cpu_baseline": cpu,
             "clocks": r64["clocks"], "gpu_launches": launches,
             "autotune": {"passes": ["y_fwd", "y_inv", "z_fwd", "z_inv", "z_fwd_kinetic_inv"],

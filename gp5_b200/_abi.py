@@ -121,6 +121,7 @@ def lib():
         "gp5cu_stepper_set_renormalization": (i, [vp, i, C.POINTER(d)]),
         "gp5cu_stepper_set_phase_constraint": (i, [vp, vp]),
         "gp5cu_stepper_set_compensation": (i, [vp, i]),
+        "gp5cu_stepper_set_stochastic_rounding": (i, [vp, C.c_int]),
         "gp5cu_stepper_advance": (i, [vp, vp, i]),
         "gp5cu_stepper_get_time": (i, [vp, C.POINTER(d)]),
         "gp5cu_stepper_set_time": (i, [vp, d]),
@@ -415,6 +416,10 @@ class Stepper:
     def set_compensation(self, on: bool) -> None:
         """Compensated complex64 state update (gp5cu_stepper_set_compensation)."""
         check(lib().gp5cu_stepper_set_compensation(self.h, 1 if on else 0))
+
+    def set_stochastic_rounding(self, on: bool) -> None:
+        """Unbiased (stochastic) rounding of the complex64 state update."""
+        check(lib().gp5cu_stepper_set_stochastic_rounding(self.h, 1 if on else 0))
 
     def set_phase_constraint(self, phase: Optional[DeviceField]) -> None:
         check(lib().gp5cu_stepper_set_phase_constraint(self.h, phase.ptr if phase is not None else None))

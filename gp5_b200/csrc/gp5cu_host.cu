@@ -883,6 +883,7 @@ int gp5cu_stepper_create(gp5cu_functional *f, int kind, double dt, int imaginary
     // gpCpp.cpp:217-224: (dt, 0) imaginary, (0, dt) real
     st->tre = imaginary ? dt : 0.0;
     st->tim = imaginary ? 0.0 : dt;
+    st->sround = p->prec == GP5_C64;  // unbiased rounding of the complex64 state update
     try {
         check_cuda(cudaMalloc(&st->Ka, p->field_bytes * p->nsolve), "cudaMalloc k buffers");
         if (kind == GP5_STEP_RK4) check_cuda(cudaMalloc(&st->Kb, p->field_bytes * p->nsolve), "cudaMalloc k buffers");
@@ -982,6 +983,18 @@ int gp5cu_stepper_set_compensation(gp5cu_stepper *st, int on) {
         st->compensate = false;
     }
     st->comp_field = nullptr;
+    GP5_CATCH
+}
+
+int gp5cu_stepper_set_stochastic_rounding(gp5cu_stepper *st, int on) {
+    GP5_TRY
+    require(st != nullptr, "stepper is NULL");
+    gp5cu_plan *p = st->func->plan;
+    if (on) require(p->prec == GP5_C64, "stochastic rounding is for complex64 plans");
+    use_device(p);
+    check_cuda(cudaStreamSynchronize(p->stream), "sync");
+    drop_graph(st);
+    st->sround = on != 0;
     GP5_CATCH
 }
 

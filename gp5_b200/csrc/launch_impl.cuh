@@ -559,6 +559,7 @@ template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) 
             P.phase_exp = (const V *)st->phase_exp;
             P.renorm_out = st->renorm ? 1 : 0;
             if (compensation_active(st)) P.comp = (__nv_bfloat162 *)st->comp;
+            P.sround = st->sround ? 1 : 0;
         }
         epilogue<Real>(p, P, last && st->renorm);
         launches += (p->ncomp == 1) ? 1 : 2;
@@ -628,6 +629,7 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
         P.phase_exp = nullptr;
         P.comp = nullptr;
         if (s == nst && compensation_active(st)) P.comp = (__nv_bfloat162 *)st->comp;
+        P.sround = st->sround ? 1 : 0;
         if (!rk4) {
             P.mode = EPI_EULER;
             P.kprev = nullptr;

@@ -270,7 +270,7 @@ template <typename Real> struct EpiParams {
     double cfac;    // stage coefficient c = tau * cfac of u~ = sigma psi - c kprev
     double dfac;    // d = tau * dfac: tau (Euler) or tau/6 (RK4)
     int turn;       // also form the next stage's transform input (stage boundary kernel)
-    int stream_aux; // psi / k loads and stores with evict-first cache hints (read once per stage)
+    int stream_aux; // psi / k (and compensation) loads and stores with evict-first cache hints
     double cnfac;   // next stage: u~' = sigma psi - (tau cnfac) k_s (RK1..RK3); psi1 for RK4/Euler
     // functional
     int fkind;
@@ -285,6 +285,9 @@ template <typename Real> struct EpiParams {
     // compensated state (complex64 real-time runs): the part of psi below FP32 resolution,
     // BF16 pairs; null = off.  psi1 = psi + (lo - d sum) is formed by a two-sum per lane
     __nv_bfloat162 *comp;
+    // complex64: the new state of the last stage (and Euler) is rounded stochastically
+    // (gp5cu_stepper_set_stochastic_rounding); ignored where comp is set
+    int sround;
 };
 
 template <typename Real>
@@ -392,12 +395,37 @@ __device__ __forceinline__ EpiIn<Real> epi_load(const EpiParams<Real> &P, long l
         in.kacc = (P.mode == EPI_RK3 || P.mode == EPI_RK4) ? P.kacc[g] : mk<Real>(0, 0);
     }
     if (P.comp && (P.mode == EPI_RK4 || P.mode == EPI_EULER)) {
-        const float2 f = __bfloat1622float2(P.comp[g]);
+        const float2 f = __bfloat1622float2(P.stream_aux ? __ldcs(P.comp + g) : P.comp[g]);
         in.lo = mk<Real>((Real)f.x, (Real)f.y);
     } else {
         in.lo = mk<Real>(0, 0);
     }
     return in;
+}
+
+// Stochastic rounding of the complex64 state update.  sround_mix is the "lowbias32" integer
+// hash (C. Wellons, 2018); sround_hash seeds it with the element index and bits of the element's
+// state and increment, so the draw differs between elements and steps, and is reproducible.
+__device__ __forceinline__ unsigned sround_mix(unsigned h) {
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    return h;
+}
+__device__ __forceinline__ unsigned sround_hash(unsigned g, unsigned a, unsigned b) {
+    return sround_mix(g * 0x9e3779b1u ^ a ^ ((b << 7) | (b >> 25)));
+}
+// r = round-to-nearest(x), lo = x - r exactly; returns r or the float next to r on lo's side,
+// the latter with probability |lo| / (its distance from r), drawn from the top 24 bits of h:
+// the expectation is x.
+__device__ __forceinline__ float sround(float r, float lo, unsigned h) {
+    if (lo == 0.f || r == 0.f || !isfinite(r)) return r;
+    const int b = __float_as_int(r);
+    const float rn = __int_as_float(((lo > 0.f) == (r > 0.f)) ? b + 1 : b - 1);
+    const float u = (float)(h >> 8) * 5.9604644775390625e-8f;  // [0, 1) in steps of 2^-24
+    return u * fabsf(rn - r) < fabsf(lo) ? rn : r;
 }
 
 // The epilogue of one site: t[c] = kinetic of u~_c (already times K^2/(2 m N^3)).
@@ -502,7 +530,22 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
             V lo;
             lo.x = (p[c].x - r.x) + delta.x;
             lo.y = (p[c].y - r.y) + delta.y;
-            P.comp[g] = __floats2bfloat162_rn((float)lo.x, (float)lo.y);
+            const __nv_bfloat162 lo2 = __floats2bfloat162_rn((float)lo.x, (float)lo.y);
+            if (P.stream_aux) __stcs(P.comp + g, lo2);
+            else P.comp[g] = lo2;
+        } else if (sizeof(Real) == 4 && P.sround) {
+            // unbiased (stochastic) rounding of p - d sum: the exact error lo of the rounded sum
+            // decides, with probability |lo| / spacing, whether the neighbouring float replaces r
+            const V delta = csub(mk<Real>(0, 0), cmul(d, sum));
+            r = cadd(p[c], delta);
+            const float lox = ((float)p[c].x - (float)r.x) + (float)delta.x;
+            const float loy = ((float)p[c].y - (float)r.y) + (float)delta.y;
+            // seeded by the element's index within its solve, so that a batched solve rounds as it
+            // does alone
+            const unsigned site = (unsigned)(i + P.nx * (j + P.ny * k)) + (unsigned)c * (unsigned)P.nsites;
+            const unsigned h = sround_hash(site, __float_as_uint((float)p[c].x), __float_as_uint((float)delta.y));
+            r.x = (Real)sround((float)r.x, lox, h);
+            r.y = (Real)sround((float)r.y, loy, sround_mix(h ^ __float_as_uint((float)p[c].y)));
         } else {
             r = csub(p[c], cmul(d, sum));
         }

@@ -128,6 +128,9 @@ struct gp5cu_stepper {
     // compensated complex64 state (gp5cu_stepper_set_compensation): BF16 pairs per element, valid
     // for the state at comp_field; active only without renormalisation and phase constraint
     bool compensate = false;
+    // complex64: stochastic rounding of the state update (gp5cu_stepper_set_stochastic_rounding;
+    // on by default for complex64 plans)
+    bool sround = false;
     void *comp = nullptr;
     void *comp_field = nullptr;
     gp5::DevScalars *ds = nullptr;          // [nsolve]
