@@ -274,12 +274,19 @@ public:
         _plan = m.plan();
         if (!_norms.empty()) check(gp5cu_stepper_set_renormalization(_st, (int)_norms.size(), _norms.data()));
         if (_compensate) check(gp5cu_stepper_set_compensation(_st, 1));
+        if (_sround >= 0) check(gp5cu_stepper_set_stochastic_rounding(_st, _sround));
     }
     // extension (no reference counterpart): compensated complex64 state update, see
     // gp5cu_stepper_set_compensation; kept across setFunctional
     void setCompensation(bool on) {
         _compensate = on;
         if (_st) check(gp5cu_stepper_set_compensation(_st, on ? 1 : 0));
+    }
+    // extension: stochastically rounded complex64 state update (the complex64 default), see
+    // gp5cu_stepper_set_stochastic_rounding; kept across setFunctional
+    void setStochasticRounding(bool on) {
+        _sround = on ? 1 : 0;
+        if (_st) check(gp5cu_stepper_set_stochastic_rounding(_st, _sround));
     }
     void setRenormalization(const std::vector<double> &normalizations) {
         _norms = normalizations;
@@ -309,6 +316,7 @@ private:
     gp5cu_plan *_plan = nullptr;
     std::vector<double> _norms;
     bool _compensate = false;
+    int _sround = -1;  // -1: the stepper's default
 };
 
 }  // namespace
@@ -352,6 +360,7 @@ PYBIND11_MODULE(gpCpp, m) {
         .def(py::init<double, std::string, bool>())
         .def("setRenormalization", &timeStepper::setRenormalization)
         .def("setCompensation", &timeStepper::setCompensation)
+        .def("setStochasticRounding", &timeStepper::setStochasticRounding)
         .def("unsetRenormalization", &timeStepper::unsetRenormalization)
         .def("setFunctional", &timeStepper::setFunctional)
         .def("advance", &timeStepper::advance)

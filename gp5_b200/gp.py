@@ -200,6 +200,11 @@ class stepper:
     def setCompensation(self, on):
         self._stepperCpp.setCompensation(bool(on))
 
+    def setStochasticRounding(self, on):
+        """Extension: stochastically rounded complex64 state update (on by default for complex64
+        fields; False rounds to nearest)."""
+        self._stepperCpp.setStochasticRounding(bool(on))
+
     def setRenormalization(self, N):
         self._stepperCpp.setRenormalization(list(N))
 
