@@ -47,10 +47,11 @@ SEED = 2024
 #   boundary 4->1: R W, psi, k3, a W psi1, W                       6
 # Five-pass path (20 launches): per stage x-fwd, y-fwd, z, y-inv, x-inv.
 MERGED_BOUNDARY = [4, 6, 7, 6]
+AXES_BOUNDARY = [4, 6, 7, 5]  # per-axis scheme: the boundary of stages 1-4 (Euler: 4)
 STAGE_XFWD = [2, 3, 3, 3]
 STAGE_XINV = [3, 5, 6, 5]
 KIND_NAMES = {0: "x_fwd_prologue", 10: "y_fwd", 22: "z_fwd_kinetic_inv", 11: "y_inv", 1: "x_inv_epilogue",
-              3: "x_stage_boundary"}
+              3: "x_stage_boundary", 12: "y_deriv", 2: "x_stage_boundary_axes"}
 
 
 def workload_geometry():
@@ -320,6 +321,22 @@ def roofline(r, dtype: str = "c128"):
                 bytes_per.append(2 * F)
             else:
                 bytes_per.append({10: F / slabs, 22: 0.0, 11: F / slabs}[k])
+    elif kinds.count(2) in (1, 4) and kinds[-1] == 2 and 3 not in kinds:
+        # per-axis kinetic scheme: per stage the y and z derivative passes (on `slabs` x-slabs)
+        # then the boundary.  One slab: y reads u and writes T (2F), z reads u and T and writes
+        # T (3F); several: a slab's u and T stay in L2 between its y and z passes, so the y pass
+        # reads u from HBM and the z pass writes T back.
+        slabs = kinds.count(12) // kinds.count(2)
+        stage = 0
+        bounds = AXES_BOUNDARY if kinds.count(2) == 4 else [4]
+        for k in kinds:
+            if k == 2:
+                bytes_per.append(bounds[stage] * F)
+                stage += 1
+            elif slabs == 1:
+                bytes_per.append({12: 2 * F, 22: 3 * F}[k])
+            else:
+                bytes_per.append(F / slabs)
     else:
         return None
     tot = {}

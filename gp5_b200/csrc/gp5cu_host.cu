@@ -434,6 +434,8 @@ gp5cu_plan *create_plan(const int shape[3], const double *const *lefts, const do
                 // slabs must split x evenly into whole tiles (x a power of two >= 32 per slab)
                 if (v >= 1 && shape[0] % v == 0 && (shape[0] / v) % 32 == 0) p->yz_slabs = v;
             }
+            const char *ks = std::getenv("GP5_KIN_SCHEME");
+            if (ks && std::string(ks) == "1") p->kin_scheme = 1;
         }
         p->nsites = (long long)shape[0] * shape[1] * shape[2];
         p->nsolve = nsolve;
@@ -920,6 +922,7 @@ int gp5cu_stepper_destroy(gp5cu_stepper *st) {
     if (st->down) cudaStreamDestroy(st->down);
     cudaFree(st->Ka);
     cudaFree(st->Kb);
+    cudaFree(st->T);
     cudaFree(st->ds);
     cudaFree(st->phase_exp);
     cudaFree(st->dstate);

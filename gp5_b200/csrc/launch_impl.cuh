@@ -570,6 +570,7 @@ template <typename Real> int Launch<Real>::step(gp5cu_stepper *st, void *field) 
 template <typename Real> void Launch<Real>::prologue(gp5cu_stepper *st, void *field) {
     using V = cpx<Real>;
     gp5cu_plan *p = st->func->plan;
+    if (p->kin_scheme == 1) return;  // the per-axis scheme's first stage reads the state itself
     OpStageIn<Real, false> in{(const V *)field, nullptr, (V *)p->work, st->ds, st->sp, 0, 0.0, 1};
     launch_axis<Real, true, MODE_FWD>(p, 0, in);
 }
@@ -583,6 +584,7 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
     using V = cpx<Real>;
     gp5cu_functional *f = st->func;
     gp5cu_plan *p = f->plan;
+    if (p->kin_scheme == 1) return step_axes(st, field);
     V *psi = (V *)field;
     V *W = (V *)p->work;
     V *Ka = (V *)st->Ka;
@@ -652,6 +654,89 @@ template <typename Real> int Launch<Real>::step_merged(gp5cu_stepper *st, void *
             launch_axis<Real, true, MODE_INV_TURN_FWD>(p, 0, op);
         }
         launches += 1 + 3 * slabs;
+    }
+    return launches;
+}
+
+// RK4 / Euler with the kinetic term as per-axis spectral second derivatives (plan kin_scheme 1).
+// Per stage s, u~_s the stage input (the state itself in the first stage, else what the
+// previous boundary wrote to the work field U, in real space):
+//   y pass    T  = IFFT_y(ky^2/(2 m Ny) FFT_y u~_s)            reads u~_s, writes T
+//   z pass    T += IFFT_z(kz^2/(2 m Nz) FFT_z u~_s)            reads u~_s and T, writes T
+//   boundary  u~_s again from psi and k_{s-1}; t = IFFT_x(kx^2/(2 m Nx) FFT_x u~_s) + T; the
+//             stage epilogue of step_merged; u~_{s+1} to U (psi1 after the last stage)
+// The three axis terms sum to the 3D operator because K^2 is separable and the axis transforms
+// commute.  Field transfers per RK4 step: 5 per stage in the y/z passes and 4 + 6 + 7 + 5 in
+// the boundaries, 42 instead of 47; 12 launches and no prologue.
+template <typename Real> int Launch<Real>::step_axes(gp5cu_stepper *st, void *field) {
+    using V = cpx<Real>;
+    gp5cu_functional *f = st->func;
+    gp5cu_plan *p = f->plan;
+    V *psi = (V *)field;
+    V *U = (V *)p->work;
+    V *Ka = (V *)st->Ka;
+    V *Kb = (V *)st->Kb;
+    // allocated in the dry pass that precedes a graph capture, or by an eager step
+    if (!st->T) check_cuda(cudaMalloc(&st->T, p->field_bytes * p->nsolve), "cudaMalloc kinetic terms");
+    V *T = (V *)st->T;
+    const bool rk4 = st->kind == GP5_STEP_RK4;
+    const int nst = rk4 ? 4 : 1;
+    const int slabs = std::max(1, p->yz_slabs);
+    const int sw = p->shape[0] / slabs;
+    int launches = 0;
+    for (int s = 1; s <= nst; s++) {
+        const V *u = s == 1 ? psi : U;
+        OpDeriv<Real, 1, false> dy{u, T, st->sp, p->shape[0], p->shape[1], p->shape[2]};
+        OpDeriv<Real, 2, true> dz{u, T, st->sp, p->shape[0], p->shape[1], p->shape[2]};
+        for (int b = 0; b < slabs; b++) {
+            if (slabs > 1) {
+                p->xr0 = b * sw;
+                p->xr_n = sw;
+            }
+            launch_axis<Real, false, MODE_FWD_MID_INV>(p, 1, dy);
+            launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, dz);
+        }
+        p->xr0 = p->xr_n = 0;
+        EpiParams<Real> P = base_epi<Real>(f);
+        P.sp = st->sp;
+        P.ds = st->ds;
+        P.psi = psi;
+        P.psi_out = psi;
+        P.kacc = Ka;
+        P.use_sigma = st->renorm ? 1 : 0;
+        P.use_alpha = st->renorm ? 1 : 0;
+        P.slot = s & 1;
+        P.u1_raw = (s == 1) ? 1 : 0;
+        P.turn = 1;
+        P.stream_aux = p->stream_aux ? 1 : 0;
+        P.renorm_out = st->renorm ? 1 : 0;
+        P.phase_exp = nullptr;
+        P.comp = nullptr;
+        if (s == nst && compensation_active(st)) P.comp = (__nv_bfloat162 *)st->comp;
+        P.sround = st->sround ? 1 : 0;
+        if (!rk4) {
+            P.mode = EPI_EULER;
+            P.kprev = nullptr;
+            P.dfac = 1.0;
+            P.phase_exp = (const V *)st->phase_exp;
+        } else {
+            P.mode = EPI_RK1 + (s - 1);
+            P.kprev = (s == 1) ? nullptr : ((s == 2) ? Ka : Kb);
+            P.kout = (s == 1) ? Ka : Kb;
+            P.dfac = 1. / 6;
+            P.cfac = (s == 1) ? 0.0 : ((s == 4) ? 1.0 : 0.5);
+            P.cnfac = (s < 4) ? ((s + 1 == 4) ? 1.0 : 0.5) : 0.0;
+            if (s == 4) P.phase_exp = (const V *)st->phase_exp;
+        }
+        V *unext = s < nst ? U : nullptr;
+        if (st->renorm) {
+            OpStageAxes<Real, true> op{P, T, unext, p->shape[0], p->shape[1], p->shape[2]};
+            launch_axis<Real, true, MODE_FWD_MID_INV>(p, 0, op);
+        } else {
+            OpStageAxes<Real, false> op{P, T, unext, p->shape[0], p->shape[1], p->shape[2]};
+            launch_axis<Real, true, MODE_FWD_MID_INV>(p, 0, op);
+        }
+        launches += 1 + 2 * slabs;
     }
     return launches;
 }

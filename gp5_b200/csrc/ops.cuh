@@ -186,6 +186,71 @@ template <typename Real> struct OpKinetic {
 // ---- stage input (prologue of the first forward pass) -----------------------------------
 // u~ = sigma_c psi - c kprev (c = tau * cfac); optional sum |u~|^2 per component ->
 // alpha_c = sqrt(N_c / (dV S)) in alpha[slot].
+// One axis's term of the kinetic operator, (1/2m)(-d^2/dx_d^2) u, in its 1D spectral form
+// IFFT_d(k_d^2 / (2 m N_d) FFT_d u): the sum of the three axes' terms is the 3D form
+// IFFT(K^2/(2 m N) FFT u) because K^2 = kx^2 + ky^2 + kz^2 and the axis transforms commute.
+// The y and z passes of the per-axis stepper scheme (Launch::step_axes) run it from the stage
+// input u into T (ACC = false) or added to T (ACC = true); the x term is formed inside the
+// stage boundary (OpStageAxes).  The factor 1/(2 m N_d) is kin * (N / N_d) with kin = 1/(2 m N).
+template <typename Real, int AXIS, bool ACC> struct OpDeriv {
+    static constexpr int NRED = 0, BATCH = ACC ? 4 : 1;
+    using Ctx = SolveCtx;
+    using V = cpx<Real>;
+    struct Pre {
+        V t;
+    };
+    const V *src;
+    V *dst;
+    const SolveParams *sp;
+    int nx, ny, nz;
+    __device__ __forceinline__ const SolveParams *params() const { return sp; }
+    __device__ __forceinline__ const DevScalars *scalars() const { return nullptr; }
+    __device__ __forceinline__ double axis_factor(const SolveParams &S, int c) const {
+        const double other = AXIS == 0 ? (double)ny * nz : (AXIS == 1 ? (double)nx * nz : (double)nx * ny);
+        return __dmul_rn(S.kin[c], other);
+    }
+    __device__ __forceinline__ V load(V x, long long, const LineRef &, double *, const SolveCtx &) const { return x; }
+    __device__ __forceinline__ V mid(V v, const LineRef &e, const SolveCtx &X) const {
+        const SolveParams &S = X.S;
+        const int pos = AXIS == 0 ? e.i : (AXIS == 1 ? e.j : e.k);
+        const double k = momentum(S, AXIS, pos, AXIS == 0 ? nx : (AXIS == 1 ? ny : nz));
+        return cscale(v, (Real)(__dmul_rn(k, k) * axis_factor(S, e.c)));
+    }
+    // z lines: the per-line part is the factor; each element forms its own kz^2
+    static constexpr bool MID_Z = true;
+    struct MidLine {
+        Real dkz;
+        double fac;
+    };
+    __device__ __forceinline__ MidLine mid_line(const LineRef &e, const SolveCtx &X) const {
+        return MidLine{(Real)X.S.dk[2], axis_factor(X.S, e.c)};
+    }
+    __device__ __forceinline__ V mid_z(V v, int kidx, const MidLine &L) const {
+        if constexpr (sizeof(Real) == 8) {
+            const double kz = __dmul_rn(L.dkz, (double)kidx);
+            return cscale(v, (Real)(__dmul_rn(kz, kz) * L.fac));
+        } else {
+            const float kz = L.dkz * (float)kidx;
+            return cscale(v, kz * kz * (float)L.fac);
+        }
+    }
+    __device__ __forceinline__ Pre pre(long long g) const {
+        Pre p;
+        if (ACC) p.t = dst[g];
+        return p;
+    }
+    __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &in, double *,
+                                         const SolveCtx &) const {
+        dst[g] = ACC ? cadd(in.t, v) : v;
+    }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const {
+        p[0] = src;
+        if (ACC) { p[1] = dst; return 2; }
+        return 1;
+    }
+    __device__ __forceinline__ void finalize(const double *, int) const {}
+};
+
 template <typename Real, bool RED> struct OpStageIn {
     static constexpr int NRED = RED ? 2 : 0, BATCH = 1;
     using Ctx = SolveCtx;
@@ -628,6 +693,74 @@ template <typename Real, bool RED, bool TURN = false> struct OpStageOut {
         p[n++] = src;
         p[n++] = P.psi;
         if (P.mode >= EPI_RK2) p[n++] = P.kprev;
+        if (P.mode == EPI_RK3 || P.mode == EPI_RK4) p[n++] = P.kacc;
+        return n;
+    }
+    __device__ __forceinline__ void finalize(const double *s, int solve) const { EpiFinalize<Real>::run(P, s, solve); }
+};
+
+#ifndef GP5_AXES_BATCH
+#define GP5_AXES_BATCH 2
+#endif
+// Stage boundary of the per-axis scheme (one component, x lines): forms the stage input
+// u~_s = sigma psi0 - c_s k_{s-1} (or the raw state in the first stage) from psi and k_{s-1},
+// its x term of the kinetic operator IFFT_x(kx^2/(2 m Nx) FFT_x u~), adds the y and z terms the
+// strided passes left in T, and runs the stage epilogue: k_s, the RK bookkeeping, and the next
+// stage's input u~_{s+1} stored in real space to unext (the last stage stores psi1 instead,
+// unext null).  The operands of u~ are read twice (before the transform and in the epilogue);
+// the second read finds the tile's lines in L2.
+template <typename Real, bool RED> struct OpStageAxes {
+    static constexpr int NRED = RED ? kNRed : 0, BATCH = GP5_AXES_BATCH;
+    static constexpr bool HEAVY_EPILOGUE = true;
+    using Ctx = SolveCtx;
+    using V = cpx<Real>;
+    struct Pre {
+        EpiIn<Real> in;
+        V t;
+    };
+    EpiParams<Real> P;
+    const V *tsum;  // y and z kinetic terms of u~_s
+    V *unext;       // u~_{s+1} (real space), or null after the last stage
+    int nx, ny, nz;
+    __device__ __forceinline__ const SolveParams *params() const { return P.sp; }
+    __device__ __forceinline__ const DevScalars *scalars() const { return P.ds; }
+    // u~_s from the psi element (src0) and k_{s-1}: the expressions of epilogue_site
+    __device__ __forceinline__ V load(V raw, long long g, const LineRef &e, double *, const SolveCtx &X) const {
+        if (P.u1_raw) return raw;
+        V x = raw;
+        if (P.use_sigma) x = cscale(x, (Real)X.sigma[e.c]);
+        if (P.mode >= EPI_RK2) {
+            V c0;
+            c0.x = (Real)(X.S.tre * P.cfac);
+            c0.y = (Real)(X.S.tim * P.cfac);
+            return csub(x, cmul(c0, P.kprev[g]));  // a normal load: the epilogue reads it again
+        }
+        return x;
+    }
+    __device__ __forceinline__ V mid(V v, const LineRef &e, const SolveCtx &X) const {
+        const SolveParams &S = X.S;
+        const double k = momentum(S, 0, e.i, nx);
+        return cscale(v, (Real)(__dmul_rn(k, k) * __dmul_rn(S.kin[e.c], (double)ny * nz)));
+    }
+    __device__ __forceinline__ Pre pre(long long g) const {
+        Pre p;
+        p.in = epi_load(P, g);
+        p.t = tsum[g];
+        return p;
+    }
+    __device__ __forceinline__ void post(long long g, const LineRef &e, V v, const Pre &in, double *acc,
+                                         const SolveCtx &X) const {
+        const V t[1] = {cadd(v, in.t)};
+        const EpiIn<Real> ins[1] = {in.in};
+        V nx_[1];
+        epilogue_site<Real, 1, RED, true>(P, X, g, e.i, e.j, e.k, t, ins, acc, nx_);
+        if (unext) unext[g] = nx_[0];
+    }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const {
+        int n = 0;
+        p[n++] = P.psi;
+        if (P.mode >= EPI_RK2) p[n++] = P.kprev;
+        p[n++] = tsum;
         if (P.mode == EPI_RK3 || P.mode == EPI_RK4) p[n++] = P.kacc;
         return n;
     }

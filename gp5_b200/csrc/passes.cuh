@@ -209,6 +209,10 @@ __device__ __forceinline__ void prefetch_aux(const TileGeom &g, long long tile, 
 }
 
 // ops that provide the hoisted z-line k-space multiply (mid_line / mid_z)
+// ops whose epilogue is long enough to run as a rolled loop (HEAVY_EPILOGUE)
+template <class Op, class = void> struct heavy_epilogue : std::false_type {};
+template <class Op> struct heavy_epilogue<Op, std::void_t<decltype(Op::HEAVY_EPILOGUE)>> : std::true_type {};
+
 template <class Op, class = void> struct has_mid_z : std::false_type {};
 template <class Op> struct has_mid_z<Op, std::void_t<decltype(Op::MID_Z)>> : std::true_type {};
 
@@ -403,6 +407,29 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 LineRef e = lr;
                 set_pos(g, e, pos);
                 op.post(lr.base + pos * g.estride, e, v[m], typename Op::Pre{}, acc, X);
+            }
+        } else if (CONTIG && heavy_epilogue<Op>::value) {
+            // a long epilogue (the per-axis stage boundary) runs as a rolled loop over the
+            // thread's own elements staged in shared memory, like the stage boundary's turn: one
+            // copy of its code.  The transform's last exchange is behind a barrier, and each
+            // thread reads back only what it wrote.
+            LayContig<N, S> lay;
+#pragma unroll
+            for (int m = 0; m < E; m++) sm[lay(line, tid + T * m)] = v[m];
+            if (lr.valid) {
+#pragma unroll 1
+                for (int m0 = 0; m0 < E; m0 += NB) {
+                    typename Op::Pre pre[NB];
+#pragma unroll
+                    for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * g.estride);
+#pragma unroll
+                    for (int j = 0; j < NB; j++) {
+                        const int pos = tid + T * (m0 + j);
+                        LineRef e = lr;
+                        set_pos(g, e, pos);
+                        op.post(lr.base + pos * g.estride, e, sm[lay(line, pos)], pre[j], acc, X);
+                    }
+                }
             }
         } else if (lr.valid) {
             // epilogue in batches: the operand loads of NB elements are issued together

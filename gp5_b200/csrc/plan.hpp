@@ -105,6 +105,10 @@ struct gp5cu_plan {
     int xr0 = 0, xr_n = 0;
     // bound of the bulk-copy ring's waits (gp5cu_plan_set_wait_bound)
     unsigned long long ring_wait_ns = GP5_RING_WAIT_DEFAULT_NS;
+    // kinetic term of the merged RK step: 0 = 3D transform (y fwd, z fwd*K^2*inv, y inv, x
+    // boundary inverse/forward); 1 = per-axis spectral second derivatives (y pass, z pass
+    // accumulating, x term inside the boundary; Launch::step_axes).  GP5_KIN_SCHEME.
+    int kin_scheme = 0;
 };
 
 struct gp5cu_functional {
@@ -125,6 +129,7 @@ struct gp5cu_stepper {
     void *phase_exp = nullptr;  // e^{i phi}, plan precision, owned
     void *Ka = nullptr, *Kb = nullptr;
     void *dstate = nullptr;  // resident state of the host-buffer entry point
+    void *T = nullptr;       // per-axis scheme: the y + z kinetic terms of the stage input
     // compensated complex64 state (gp5cu_stepper_set_compensation): BF16 pairs per element, valid
     // for the state at comp_field; active only without renormalisation and phase constraint
     bool compensate = false;
@@ -174,6 +179,7 @@ template <typename Real> struct Launch {
     static void convert(gp5cu_plan *p, const double *in128, void *out, const void *in, double *out128, long long n);
     static int step(gp5cu_stepper *st, void *field);  // queue one step; returns launches
     static int step_merged(gp5cu_stepper *st, void *field, bool prologue);
+    static int step_axes(gp5cu_stepper *st, void *field);  // step_merged's per-axis scheme
     static void prologue(gp5cu_stepper *st, void *field);  // forward x transform of psi
     static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
     // times every tile shape (and, with radix, both radix schedules) of the strided y/z passes
