@@ -283,6 +283,8 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
     V *sm = reinterpret_cast<V *>(smem_raw);
 
     pdl_enter();
+    // x lines are contiguous: a compile-time unit stride spares the 64-bit multiplies
+    const long long es = CONTIG ? 1LL : g.estride;
     int tid, line;
     if (CONTIG) { tid = threadIdx.x % T; line = threadIdx.x / T; }
     else { line = threadIdx.x % LINES; tid = threadIdx.x / LINES; }
@@ -305,7 +307,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
         V v[E];
 #pragma unroll
         for (int m = 0; m < E; m++)
-            v[m] = lr.valid ? src0[lr.base + (tid + T * m) * g.estride] : mk<Real>(0, 0);
+            v[m] = lr.valid ? src0[lr.base + (tid + T * m) * es] : mk<Real>(0, 0);
         if (op.params() || op.scalars()) {  // uniform: ops without per-solve data skip the barrier
             ctx_store(X, op.params(), op.scalars(), cw);
             __syncthreads();
@@ -317,7 +319,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 const int pos = tid + T * m;
                 LineRef e = lr;
                 set_pos(g, e, pos);
-                const long long ge = lr.base + pos * g.estride;
+                const long long ge = lr.base + pos * es;
                 v[m] = op.load(v[m], ge, e, acc, X);
             }
         }
@@ -336,14 +338,14 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 for (int m0 = 0; m0 < E; m0 += NB) {
                     typename Op::Pre pre[NB];
 #pragma unroll
-                    for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * g.estride);
+                    for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * es);
 #pragma unroll
                     for (int j = 0; j < NB; j++) {
                         const int pos = tid + T * (m0 + j);
                         LineRef e = lr;
                         set_pos(g, e, pos);
                         const int si = lay(line, pos);
-                        sm[si] = op.turn(lr.base + pos * g.estride, e, sm[si], pre[j], acc, X);
+                        sm[si] = op.turn(lr.base + pos * es, e, sm[si], pre[j], acc, X);
                     }
                 }
             }
@@ -406,7 +408,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 const int pos = tid + T * m;
                 LineRef e = lr;
                 set_pos(g, e, pos);
-                op.post(lr.base + pos * g.estride, e, v[m], typename Op::Pre{}, acc, X);
+                op.post(lr.base + pos * es, e, v[m], typename Op::Pre{}, acc, X);
             }
         } else if (CONTIG && heavy_epilogue<Op>::value) {
             // a long epilogue (the per-axis stage boundary) runs as a rolled loop over the
@@ -421,13 +423,13 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                 for (int m0 = 0; m0 < E; m0 += NB) {
                     typename Op::Pre pre[NB];
 #pragma unroll
-                    for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * g.estride);
+                    for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * es);
 #pragma unroll
                     for (int j = 0; j < NB; j++) {
                         const int pos = tid + T * (m0 + j);
                         LineRef e = lr;
                         set_pos(g, e, pos);
-                        op.post(lr.base + pos * g.estride, e, sm[lay(line, pos)], pre[j], acc, X);
+                        op.post(lr.base + pos * es, e, sm[lay(line, pos)], pre[j], acc, X);
                     }
                 }
             }
@@ -437,13 +439,13 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
             for (int m0 = 0; m0 < E; m0 += NB) {
                 typename Op::Pre pre[NB];
 #pragma unroll
-                for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * g.estride);
+                for (int j = 0; j < NB; j++) pre[j] = op.pre(lr.base + (tid + T * (m0 + j)) * es);
 #pragma unroll
                 for (int j = 0; j < NB; j++) {
                     const int pos = tid + T * (m0 + j);
                     LineRef e = lr;
                     set_pos(g, e, pos);
-                    op.post(lr.base + pos * g.estride, e, v[m0 + j], pre[j], acc, X);
+                    op.post(lr.base + pos * es, e, v[m0 + j], pre[j], acc, X);
                 }
             }
         }
