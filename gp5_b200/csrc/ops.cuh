@@ -493,6 +493,26 @@ __device__ __forceinline__ float sround(float r, float lo, unsigned h) {
     return u * fabsf(rn - r) < fabsf(lo) ? rn : r;
 }
 
+// Stage constants of the epilogue in the plan precision: c0 = tau cfac (u~_s = sigma psi0 -
+// c0 k_{s-1}), cn = tau cnfac (u~_{s+1}), d = tau dfac (psi1 = p - d sum).  The stage boundary
+// forms them once per tile (its element loop would otherwise repeat the FP64 products, since
+// the compiler cannot keep the shared-memory context in registers across the loop's shared
+// stores); the other callers form them per site.
+template <typename Real> struct StageK {
+    cpx<Real> c0, cn, d;
+};
+template <typename Real>
+__device__ __forceinline__ StageK<Real> stage_k(const EpiParams<Real> &P, const SolveParams &S) {
+    StageK<Real> K;
+    K.c0.x = (Real)(S.tre * P.cfac);
+    K.c0.y = (Real)(S.tim * P.cfac);
+    K.cn.x = (Real)(S.tre * P.cnfac);
+    K.cn.y = (Real)(S.tim * P.cnfac);
+    K.d.x = (Real)(S.tre * P.dfac);
+    K.d.y = (Real)(S.tim * P.dfac);
+    return K;
+}
+
 // The epilogue of one site: t[c] = kinetic of u~_c (already times K^2/(2 m N^3)).
 // With P.turn the epilogue also returns, in next[c], the input of the following transform:
 // u~_{s+1} = sigma psi - cn k_s after stages 1-3, or the new state psi1 after the last stage
@@ -500,7 +520,7 @@ __device__ __forceinline__ float sround(float r, float lo, unsigned h) {
 template <typename Real, int NC, bool RED, bool TURN = false>
 __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const SolveCtx &X, long long s, int i,
                                               int j, int k, const cpx<Real> (&t)[NC], const EpiIn<Real> (&in)[NC],
-                                              double *acc, cpx<Real> (&next)[NC]) {
+                                              double *acc, cpx<Real> (&next)[NC], const StageK<Real> &K) {
     using V = cpx<Real>;
     const SolveParams &S = X.S;
     V p[NC], u[NC], kin[NC], h[NC];
@@ -513,12 +533,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
         if (P.use_sigma) x = cscale(x, (Real)X.sigma[c]);
         p[c] = x;
         V ut = P.u1_raw ? raw : x;
-        if (mode >= EPI_RK2) {
-            V c0;
-            c0.x = (Real)(S.tre * P.cfac);
-            c0.y = (Real)(S.tim * P.cfac);
-            ut = csub(x, cmul(c0, in[c].kprev));
-        }
+        if (mode >= EPI_RK2) ut = csub(x, cmul(K.c0, in[c].kprev));
         if (P.use_alpha) {
             const Real a = (Real)X.alpha[P.slot][c];
             u[c] = cscale(ut, a);
@@ -568,10 +583,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
                 aux_store(P, P.kout + g, h[c]);
             }
             if (TURN) {
-                V cn;
-                cn.x = (Real)(S.tre * P.cnfac);
-                cn.y = (Real)(S.tim * P.cnfac);
-                const V nx = csub(p[c], cmul(cn, h[c]));
+                const V nx = csub(p[c], cmul(K.cn, h[c]));
                 next[c] = nx;
                 if (RED) acc[c] += (double)nx.x * (double)nx.x + (double)nx.y * (double)nx.y;
             }
@@ -579,9 +591,7 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
         return;
     }
     // EULER / RK4: psi1 = p - d * (sum)
-    V d;
-    d.x = (Real)(S.tre * P.dfac);
-    d.y = (Real)(S.tim * P.dfac);
+    const V d = K.d;
 #pragma unroll
     for (int c = 0; c < NC; c++) {
         const long long g = s + (long long)c * P.nsites;
@@ -669,12 +679,13 @@ template <typename Real, bool RED, bool TURN = false> struct OpStageOut {
     __device__ __forceinline__ V load(V x, long long, const LineRef &, double *, const SolveCtx &) const { return x; }
     __device__ __forceinline__ V mid(V v, const LineRef &, const SolveCtx &) const { return v; }
     __device__ __forceinline__ Pre pre(long long g) const { return epi_load(P, g); }
+    __device__ __forceinline__ StageK<Real> consts(const SolveCtx &X) const { return stage_k(P, X.S); }
     __device__ __forceinline__ V turn(long long g, const LineRef &e, V v, const Pre &in, double *acc,
-                                      const SolveCtx &X) const {
+                                      const SolveCtx &X, const StageK<Real> &K) const {
         const V t[1] = {v};
         const Pre ins[1] = {in};
         V nx[1] = {v};
-        epilogue_site<Real, 1, RED, true>(P, X, g, e.i, e.j, e.k, t, ins, acc, nx);
+        epilogue_site<Real, 1, RED, true>(P, X, g, e.i, e.j, e.k, t, ins, acc, nx, K);
         return nx[0];
     }
     __device__ __forceinline__ void post(long long g, const LineRef &e, V v, const Pre &in, double *acc,
@@ -685,7 +696,7 @@ template <typename Real, bool RED, bool TURN = false> struct OpStageOut {
             const V t[1] = {v};
             const Pre ins[1] = {in};
             V nx[1];
-            epilogue_site<Real, 1, RED>(P, X, g, e.i, e.j, e.k, t, ins, acc, nx);
+            epilogue_site<Real, 1, RED>(P, X, g, e.i, e.j, e.k, t, ins, acc, nx, stage_k(P, X.S));
         }
     }
     __device__ __forceinline__ int streams(const void *(&p)[4]) const {
@@ -753,7 +764,7 @@ template <typename Real, bool RED> struct OpStageAxes {
         const V t[1] = {cadd(v, in.t)};
         const EpiIn<Real> ins[1] = {in.in};
         V nx_[1];
-        epilogue_site<Real, 1, RED, true>(P, X, g, e.i, e.j, e.k, t, ins, acc, nx_);
+        epilogue_site<Real, 1, RED, true>(P, X, g, e.i, e.j, e.k, t, ins, acc, nx_, stage_k(P, X.S));
         if (unext) unext[g] = nx_[0];
     }
     __device__ __forceinline__ int streams(const void *(&p)[4]) const {
@@ -790,7 +801,7 @@ template <typename Real, int NC, bool RED> struct OpSiteEpilogue {
         const long long r = s / P.nx;
         const int j = (int)(r % P.ny), k = (int)(r / P.ny);
         V nx[NC];
-        epilogue_site<Real, NC, RED>(P, X, g0, i, j, k, t, in, acc, nx);
+        epilogue_site<Real, NC, RED>(P, X, g0, i, j, k, t, in, acc, nx, stage_k(P, X.S));
     }
     __device__ __forceinline__ void finalize(const double *s, int solve) const { EpiFinalize<Real>::run(P, s, solve); }
 };

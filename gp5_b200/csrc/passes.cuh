@@ -334,6 +334,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
 #pragma unroll
             for (int m = 0; m < E; m++) sm[lay(line, tid + T * m)] = v[m];
             if (lr.valid) {
+                const auto K = op.consts(X);  // once per tile, out of the element loop
 #pragma unroll 1
                 for (int m0 = 0; m0 < E; m0 += NB) {
                     typename Op::Pre pre[NB];
@@ -345,7 +346,7 @@ k_axis_reg(const TileGeom g, Op op, const cpx<Real> *__restrict__ tw, const RedS
                         LineRef e = lr;
                         set_pos(g, e, pos);
                         const int si = lay(line, pos);
-                        sm[si] = op.turn(lr.base + pos * es, e, sm[si], pre[j], acc, X);
+                        sm[si] = op.turn(lr.base + pos * es, e, sm[si], pre[j], acc, X, K);
                     }
                 }
             }

@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(RingTile<Real, N, S>::THREADS, 1)
         for (int m = 0; m < E; m++) sm[lay(line, tid + T * m)] = v[m];
         if (lr.valid && active) {
             // the stage epilogue, operands from the ring (streams 1..3: psi, k_{s-1}, accumulator)
+            const StageK<Real> K = op.consts(X);
 #pragma unroll 1
             for (int m0 = 0; m0 < E; m0 += NB) {
 #pragma unroll
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(RingTile<Real, N, S>::THREADS, 1)
                     LineRef e = lr;
                     set_pos(g, e, pos);
                     const int si = lay(line, pos);
-                    sm[si] = op.turn(lr.base + pos, e, sm[si], in, acc, X);
+                    sm[si] = op.turn(lr.base + pos, e, sm[si], in, acc, X, K);
                 }
             }
         }
