@@ -548,7 +548,8 @@ __device__ __forceinline__ void epilogue_site(const EpiParams<Real> &P, const So
     if (!TURN && (mode == EPI_H || mode == EPI_OBS)) {
 #pragma unroll
         for (int c = 0; c < NC; c++) P.kout[s + (long long)c * P.nsites] = h[c];
-        if (RED && mode == EPI_OBS) {
+        // (compiled only where the caller provides all eight sums: the stage boundary has two)
+        if constexpr (RED && !TURN) if (mode == EPI_OBS) {
 #pragma unroll
             for (int c = 0; c < NC; c++) {
                 const double ur = u[c].x, ui = u[c].y;
@@ -668,7 +669,9 @@ template <typename Real> struct EpiFinalize {
 // BATCH = 4: the epilogue issues the psi / k loads of four elements together (the boundary
 // waits on memory; 4 measured 8% faster than 2 at 256^3, 8 spills).
 template <typename Real, bool RED, bool TURN = false> struct OpStageOut {
-    static constexpr int NRED = RED ? kNRed : 0, BATCH = 4;
+    // the stage boundary only reduces |next|^2 per component (two sums); the observables
+    // epilogue needs all eight
+    static constexpr int NRED = RED ? (TURN ? 2 : kNRed) : 0, BATCH = 4;
     using Ctx = SolveCtx;
     using V = cpx<Real>;
     using Pre = EpiIn<Real>;
