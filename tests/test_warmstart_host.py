@@ -135,3 +135,26 @@ def test_free_profile_recovers_the_isolated_profile():
     got, k = ws.free_profile(axis, N)
     assert 0.5 * kappa < k < 1.5 * kappa  # log-slope estimate (the core still leaks into it)
     assert np.max(np.abs(got - samples_iso)) < 1e-5 * np.max(samples_iso)
+
+
+def test_lsq_samples_recover_an_image_sum_placement():
+    """A field that is itself a profile_start placement is fitted: the least-squares samples
+    place back onto the same field (32^3, a flat-topped droplet-like profile; the round trip
+    re-estimates the tail rate, hence not to rounding)."""
+    N, n = 60.0, 32
+    r = ws.radii(N)
+    R0 = 0.6 * N ** (1.0 / 3.0)
+    s0 = 0.9 / (1.0 + np.exp((r - R0) / 0.5))  # flat top with a smooth edge
+    psi = ws.profile_start(s0, N, n)
+    s1 = ws.lsq_samples(psi, N)
+    back = ws.profile_start(s1, N, n)
+    assert np.max(np.abs(back - psi)) <= 1e-4 * np.max(np.abs(psi))
+
+
+def test_lsq_samples_fit_better_than_the_axis_samples():
+    """For a field that is not an image sum (a Gaussian product), the least-squares samples
+    place closer to it than its own axis samples do."""
+    N, n = 60.0, 32
+    psi = ws.gaussian_start(N, n, None)
+    err = lambda s: float(np.sqrt(np.mean(np.abs(ws.profile_start(s, N, n) - psi) ** 2)))
+    assert err(ws.lsq_samples(psi, N)) <= err(ws.radial_samples(psi, N))
