@@ -297,6 +297,99 @@ def run_ours(args, rank, world, local_rank):
     return results, launches
 
 
+def cufft_comparator(dev: int, steps: int = 10, warmup: int = 3) -> dict:
+    """cuFFT, through torch.fft, as a timed comparator (never the product path).
+
+    On the bench workload, per precision: (1) one 3D forward + inverse transform pair of the
+    256^3 field by cuFFT against gp5cu_fft's pair; (2) the product's RK4 step (stepper.cpp:46-71
+    with the LHY functional, functional.cpp:105-122, and the laplacian of operators.cpp:28-36)
+    written as unfused torch operations around cuFFT, timed per step, with its one-step
+    difference from the product's step (relative to max |psi|).  CUDA events on the stream the
+    work is queued on; inputs larger than L2."""
+    import numpy as np
+    import torch
+
+    from gp5_b200 import _abi
+
+    shape, left, right = workload_geometry()
+    n = shape[0]
+    L = right[0] - left[0]
+    psi0 = initial_state()
+    stream = torch.cuda.Stream(device=dev)
+    out = {"note": "library comparator: cuFFT via torch.fft plus unfused torch element-wise kernels",
+           "steps": steps}
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for key, prec, cdt, rdt in (("c128", _abi.GP5_C128, torch.complex128, torch.float64),
+                                ("c64", _abi.GP5_C64, torch.complex64, torch.float32)):
+        with torch.cuda.stream(stream):
+            # the field's x-fastest layout is a C-order (z, y, x) tensor
+            x0 = torch.from_numpy(np.ascontiguousarray(psi0[..., 0].transpose(2, 1, 0))).to(dev).to(cdt)
+            m = torch.fft.fftfreq(n, d=1.0 / n, dtype=torch.float64, device=f"cuda:{dev}")
+            k2 = ((2 * math.pi / L) * m) ** 2
+            K2 = ((k2[None, None, :] + k2[None, :, None]) + k2[:, None, None]).to(rdt)
+            tau = 1j * DT  # real time: the step is (0, dt)
+
+            def H(u):
+                lap = torch.fft.ifftn(torch.fft.fftn(u) * (-K2))  # ifftn carries the 1/N^3
+                dens = u.real * u.real + u.imag * u.imag
+                return -0.5 * lap + (C3 * dens + C4 * dens * torch.sqrt(dens)) * u
+
+            def rk4(psi):
+                k1 = H(psi)
+                k2_ = H(psi - (tau * 0.5) * k1)
+                k3 = H(psi - (tau * 0.5) * k2_)
+                k4 = H(psi - tau * k3)
+                return psi - ((1.0 / 6.0) * tau) * (((k1 + 2 * k2_) + 2 * k3) + k4)
+
+            one = rk4(x0)
+            state = {"psi": x0}
+
+            def run():
+                state["psi"] = rk4(state["psi"])
+
+            for _ in range(warmup):
+                run()
+            ms_step = timed(run, steps)
+            fft_ms = timed(lambda: torch.fft.ifftn(torch.fft.fftn(x0)), steps)
+            one_host = one.cpu().numpy()
+            del state, one
+        # the product on the same stream: a plan, the forward + inverse pair, one RK4 step
+        plan = _abi.Plan(shape, left, right, precision=prec, device=dev)
+        plan.set_stream(stream.cuda_stream)
+        src, dst = plan.field(psi0), plan.field()
+
+        def pair():
+            plan.fft(src, dst, _abi.GP5_FORWARD)
+            plan.fft(dst, dst, _abi.GP5_BACKWARD)
+
+        for _ in range(warmup):
+            pair()
+        ours_fft_ms = timed(pair, steps)
+        func = _abi.Functional(plan, _abi.GP5_FUNC_LHY, c3=C3, c4=C4)
+        st = _abi.Stepper(func, DT, _abi.GP5_STEP_RK4, imaginary=False)
+        f = plan.field(psi0)
+        st.advance(f, 1)
+        mine = f.download()[..., 0].transpose(2, 1, 0)
+        diff = float(np.max(np.abs(mine - one_host)) / np.max(np.abs(one_host)))
+        out[key] = {"rk4_ms_per_step": ms_step, "value": n ** 3 / (ms_step / 1e3), "unit": "site-updates/s",
+                    "fft3d_pair_ms": {"cufft": fft_ms, "gp5cu_fft": ours_fft_ms},
+                    "one_step_rel_diff_vs_product": diff}
+        del f, st, func, src, dst, plan, x0, K2
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
+
+
 def roofline(r, dtype: str = "c128"):
     """Dominant kernel (largest share of a step) with its algorithmic bytes per launch."""
     prof = r["profile"]
@@ -696,6 +789,8 @@ def main():
                     help="also run the complex64-vs-complex128 quench report and write it here")
     ap.add_argument("--batch", type=int, default=64,
                     help="solves of the ground-state leg, in complex128 and in complex64 (0: skip)")
+    ap.add_argument("--no-comparator", action="store_true",
+                    help="skip the cuFFT comparator (torch.fft RK4 step and transform pair)")
     ap.add_argument("--case", choices=["step64", "step128", "obs128", "cluster"],
                     help="run one small profiling case of the workload and exit (no JSON line)")
     args = ap.parse_args()
@@ -745,6 +840,9 @@ def main():
         per_rank = max(1, args.batch // world)
         gs = run_batch(per_rank, local_rank, rank=rank, world=world, precision="c128")
         gs["c64"] = run_batch(per_rank, local_rank, rank=rank, world=world, precision="c64")
+    comparator = None
+    if world == 1 and not args.no_comparator:
+        comparator = cufft_comparator(local_rank)
     prep = None
     if args.precision_report and world == 1:
         prep = precision_report(local_rank)
@@ -798,6 +896,10 @@ def main():
             "autotune": {"passes": ["y_fwd", "y_inv", "z_fwd", "z_inv", "z_fwd_kinetic_inv"],
                          "threads_per_cta": {"c128": r64["tiles"], "c64": r32["tiles"]}}, "ground_states": gs,
             "launches_per_step": r64["launches_per_step"]}
+    if comparator is not None:
+        for key, r in (("c128", r64), ("c64", r32)):
+            comparator[key]["product_over_comparator"] = r["value"] / comparator[key]["value"]
+        line["cufft_comparator"] = comparator
     print(json.dumps(line))
 
 

@@ -111,6 +111,7 @@ def lib():
         "gp5cu_norm": (i, [vp, vp, i, C.POINTER(d)]),
         "gp5cu_normalize": (i, [vp, vp, i, d]),
         "gp5cu_max_density": (i, [vp, vp, C.POINTER(d)]),
+        "gp5cu_init_gaussian": (i, [vp, vp, i, C.POINTER(d)]),
         "gp5cu_functional_desc_init": (None, [C.POINTER(FunctionalDesc)]),
         "gp5cu_functional_create": (i, [vp, C.POINTER(FunctionalDesc), pp]),
         "gp5cu_functional_destroy": (i, [vp]),
@@ -230,6 +231,11 @@ class Plan:
 
     def normalize(self, f: "DeviceField", N: float, comp: int = 0) -> None:
         check(lib().gp5cu_normalize(self.h, f.ptr, comp, float(N)))
+
+    def init_gaussian(self, f: "DeviceField", sigma, comp: int = 0) -> None:
+        """f[..., comp] = exp(-sum_d x_d^2 / (2 sigma_d^2)) on the device (gp5cu_init_gaussian)."""
+        sig = (float(sigma),) * 3 if np.isscalar(sigma) else tuple(float(v) for v in sigma)
+        check(lib().gp5cu_init_gaussian(self.h, f.ptr, comp, (C.c_double * 3)(*sig)))
 
     def max_density(self, f: "DeviceField") -> float:
         out = C.c_double()

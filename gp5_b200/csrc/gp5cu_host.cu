@@ -742,6 +742,18 @@ int gp5cu_normalize(gp5cu_plan *p, void *field, int comp, double N) {
     GP5_CATCH
 }
 
+int gp5cu_init_gaussian(gp5cu_plan *p, void *field, int comp, const double sigma[3]) {
+    GP5_TRY
+    require(p && sigma, "NULL argument");
+    check_field_ptr(field, "field");
+    require(comp >= 0 && comp < p->ncomp, "component out of range");
+    require(p->nsolve == 1, "plan carries several solves");
+    for (int q = 0; q < 3; q++) require(sigma[q] > 0 && std::isfinite(sigma[q]), "widths must be positive and finite");
+    use_device(p);
+    dispatch(p, [&](auto r) { Launch<decltype(r)>::init_gaussian(p, field, comp, sigma); });
+    GP5_CATCH
+}
+
 int gp5cu_max_density(gp5cu_plan *p, const void *field, double *out) {
     GP5_TRY
     require(p && out, "NULL argument");

@@ -241,6 +241,25 @@ __global__ void __launch_bounds__(256) k_max_density(const cpx<Real> *f, long lo
     }
 }
 
+// psi_c = exp(-(ax x^2 + ay y^2 + az z^2)) + 0i at the cell centres x = left + (i + 1/2) dx
+// (initGaussian, src/geometry.cpp:251-276); arithmetic in FP64, rounded to Real once.
+template <typename Real>
+__global__ void __launch_bounds__(256) k_init_gaussian(cpx<Real> *f, int nx, int ny, long long nsites, double x0,
+                                                       double y0, double z0, double dx, double dy, double dz,
+                                                       double ax, double ay, double az) {
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nsites;
+         s += (long long)gridDim.x * blockDim.x) {
+        const long long jk = s / nx;
+        const int i = (int)(s - jk * nx), j = (int)(jk % ny), k = (int)(jk / ny);
+        // uncontracted, in the reference's order: only exp() rounds differently from the host
+        const double x = __dadd_rn(x0, __dmul_rn(i + 0.5, dx)), y = __dadd_rn(y0, __dmul_rn(j + 0.5, dy)),
+                     z = __dadd_rn(z0, __dmul_rn(k + 0.5, dz));
+        const double t = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(ax, x), x), __dmul_rn(__dmul_rn(ay, y), y)),
+                                   __dmul_rn(__dmul_rn(az, z), z));
+        f[s] = mk<Real>((Real)exp(-t), (Real)0);
+    }
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(256) k_phase_exp(const Real *phase, cpx<Real> *out, long long n) {
     for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < n;
@@ -487,6 +506,19 @@ void Launch<Real>::convert(gp5cu_plan *p, const double *in128, void *out, const 
     OpConvert<Real> op{(const double2 *)in128, (cpx<Real> *)out, (const cpx<Real> *)in, (double2 *)out128};
     k_pointwise<OpConvert<Real>><<<p->pw_blocks, kThreads, 0, p->stream>>>(n, p->pw_blocks, op, red_slot(p));
     check_cuda(cudaGetLastError(), "convert launch");
+}
+
+template <typename Real> void Launch<Real>::init_gaussian(gp5cu_plan *p, void *field, int comp, const double sigma[3]) {
+    double a[3], d[3];
+    for (int q = 0; q < 3; q++) {
+        a[q] = 1.0 / (2 * sigma[q] * sigma[q]);
+        d[q] = (p->right[q] - p->left[q]) / p->shape[q];
+    }
+    cpx<Real> *f = (cpx<Real> *)field + (long long)comp * p->nsites;
+    k_init_gaussian<Real><<<p->pw_blocks, kThreads, 0, p->stream>>>(f, p->shape[0], p->shape[1], p->nsites,
+                                                                     p->left[0], p->left[1], p->left[2], d[0],
+                                                                     d[1], d[2], a[0], a[1], a[2]);
+    check_cuda(cudaGetLastError(), "init_gaussian launch");
 }
 
 template <typename Real> void Launch<Real>::phase_exp(gp5cu_plan *p, const void *phase, void *out) {

@@ -182,6 +182,7 @@ template <typename Real> struct Launch {
     static int step_axes(gp5cu_stepper *st, void *field);  // step_merged's per-axis scheme
     static void prologue(gp5cu_stepper *st, void *field);  // forward x transform of psi
     static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
+    static void init_gaussian(gp5cu_plan *p, void *field, int comp, const double sigma[3]);
     // times every tile shape (and, with radix, both radix schedules) of the strided y/z passes
     // on the zeroed work field, and with radix both schedules of the stage boundary; keeps the
     // fastest in p->tile_threads, p->radix and p->radix_boundary

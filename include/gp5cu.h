@@ -102,6 +102,9 @@ int gp5cu_laplacian(gp5cu_plan *plan, const void *dsrc, void *ddst);
 int gp5cu_norm(gp5cu_plan *plan, const void *dfield, int comp, double *out);
 /* gp::normalize (src/geometry.cpp:217-229): psi_c *= sqrt(N / norm_c). */
 int gp5cu_normalize(gp5cu_plan *plan, void *dfield, int comp, double N);
+/* gp::initGaussian (src/geometry.cpp:251-276): psi_comp = exp(-sum_d x_d^2 / (2 sigma_d^2)) + 0i
+ * at the cell centres; the other components are left as they are.  Single-solve plans. */
+int gp5cu_init_gaussian(gp5cu_plan *plan, void *dfield, int comp, const double sigma[3]);
 /* gp.maxDensity (python/gp/gp.py:210-222): max |psi|^2 over all sites and components. */
 int gp5cu_max_density(gp5cu_plan *plan, const void *dfield, double *out);
 

@@ -38,6 +38,30 @@ def make(abi, shape, left=(-1, -1, -1), right=(1, 1, 1), ncomp=1, prec=0):
     return abi.Plan(shape, left, right, ncomp=ncomp, precision=prec)
 
 
+# ---------------------------------------------------------------- initial state
+@pytest.mark.parametrize("prec,tol", [(0, 1e-15), (1, 1e-7)])
+def test_init_gaussian_vs_oracle(abi, prec, tol):
+    """gp5cu_init_gaussian against the oracle's initGaussian (geometry.cpp:251-276) on an
+    anisotropic box and widths; the other component keeps its values."""
+    geo = o.Geometry((30, 20, 17), (-10.0, -6.0, -3.5), (10.0, 8.0, 4.0))
+    sigma = (5.0, 2.5, 1.25)
+    p = make(abi, geo.shape, geo.left, geo.right, ncomp=2, prec=prec)
+    start = rand_field(geo.shape, 11, ncomp=2)
+    f = p.field(start)
+    p.init_gaussian(f, sigma, comp=0)
+    got = f.download()
+    ref = start.copy()
+    o.init_gaussian(geo, sigma, ref, comp=0)
+    assert rel(got[..., 0], ref[..., 0]) < tol
+    assert np.all(got[..., 0].imag == 0)
+    if prec == 0:
+        assert np.array_equal(got[..., 1], ref[..., 1])
+    else:
+        assert rel(got[..., 1], ref[..., 1]) < 1e-7
+    with pytest.raises(abi.Gp5Error):
+        p.init_gaussian(f, (1.0, 0.0, 1.0))
+
+
 # ---------------------------------------------------------------- transforms
 @pytest.mark.parametrize("prec,tol", [(0, 1e-13), (1, 2e-6)])
 def test_fft_golden_mixed_radix(abi, prec, tol):
