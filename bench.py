@@ -270,7 +270,7 @@ def run_ours(args, rank, world, local_rank):
                 # and downloaded, with the copies of neighbouring states overlapping the steps
                 ins = [host_in.data_ptr()] * n_e2e
                 outs = [(host_out if k % 2 == 0 else host_out2).data_ptr() for k in range(n_e2e)]
-                st.advance_host_many(ins[:2], outs[:2], 1)  # warm (captures the second state's graph)
+                st.advance_host_many(ins[:3], outs[:3], 1)  # warm (captures the device states' graphs)
                 torch.cuda.synchronize()
                 if world > 1:
                     torch.distributed.barrier()

@@ -925,7 +925,7 @@ int gp5cu_stepper_destroy(gp5cu_stepper *st) {
     drop_graph(st);
     if (st->up) cudaStreamSynchronize(st->up);
     if (st->down) cudaStreamSynchronize(st->down);
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < gp5cu_stepper::kHostStates; b++) {
         if (st->ev_up[b]) cudaEventDestroy(st->ev_up[b]);
         if (st->ev_done[b]) cudaEventDestroy(st->ev_done[b]);
         if (st->ev_down[b]) cudaEventDestroy(st->ev_down[b]);
@@ -938,7 +938,7 @@ int gp5cu_stepper_destroy(gp5cu_stepper *st) {
     cudaFree(st->ds);
     cudaFree(st->phase_exp);
     cudaFree(st->dstate);
-    cudaFree(st->dstate2);
+    for (void *d : st->dstate_more) cudaFree(d);
     cudaFree(st->comp);
     cudaFree(st->sp);
     delete st;
@@ -950,9 +950,11 @@ void drop_graph(gp5cu_stepper *st) {
     if (st->exec) cudaGraphExecDestroy(st->exec);
     st->exec = nullptr;
     st->graph_field = nullptr;
-    if (st->exec_alt) cudaGraphExecDestroy(st->exec_alt);
-    st->exec_alt = nullptr;
-    st->graph_field_alt = nullptr;
+    for (int a = 0; a < gp5cu_stepper::kAltGraphs; a++) {
+        if (st->exec_alt[a]) cudaGraphExecDestroy(st->exec_alt[a]);
+        st->exec_alt[a] = nullptr;
+        st->graph_field_alt[a] = nullptr;
+    }
 }
 }  // extern "C++"
 
@@ -1092,8 +1094,8 @@ void capture_graph(gp5cu_stepper *st, void *field, bool merged, int ksteps) {
 }
 }  // extern "C++"
 
-// Queues nsteps steps of `field` on the plan stream (no synchronisation).  The two most recent
-// fields keep their captured one-step graphs.
+// Queues nsteps steps of `field` on the plan stream (no synchronisation).  The three most
+// recent fields keep their captured one-step graphs.
 static void enqueue_advance(gp5cu_stepper *st, void *field, int nsteps) {
     gp5cu_plan *p = st->func->plan;
     const bool merged = merged_path(p);
@@ -1104,18 +1106,35 @@ static void enqueue_advance(gp5cu_stepper *st, void *field, int nsteps) {
     }
     auto fits = [&](cudaGraphExec_t e, void *f, bool m, int k) { return e && f == field && m == merged && k == 1; };
     if (!fits(st->exec, st->graph_field, st->graph_merged, st->graph_steps)) {
-        if (fits(st->exec_alt, st->graph_field_alt, st->graph_merged_alt, st->graph_steps_alt)) {
-            std::swap(st->exec, st->exec_alt);
-            std::swap(st->graph_field, st->graph_field_alt);
-            std::swap(st->graph_merged, st->graph_merged_alt);
-            std::swap(st->graph_steps, st->graph_steps_alt);
+        constexpr int NA = gp5cu_stepper::kAltGraphs;
+        int hit = -1;
+        for (int a = 0; a < NA && hit < 0; a++)
+            if (fits(st->exec_alt[a], st->graph_field_alt[a], st->graph_merged_alt[a], st->graph_steps_alt[a])) hit = a;
+        // least recently used last: a hit leaves its slot, a miss drops the last one
+        const int from = hit >= 0 ? hit : NA - 1;
+        cudaGraphExec_t e = st->exec_alt[from];
+        void *f = st->graph_field_alt[from];
+        const bool m = st->graph_merged_alt[from];
+        const int k = st->graph_steps_alt[from];
+        if (hit < 0 && e) cudaGraphExecDestroy(e);
+        for (int a = from; a > 0; a--) {
+            st->exec_alt[a] = st->exec_alt[a - 1];
+            st->graph_field_alt[a] = st->graph_field_alt[a - 1];
+            st->graph_merged_alt[a] = st->graph_merged_alt[a - 1];
+            st->graph_steps_alt[a] = st->graph_steps_alt[a - 1];
+        }
+        st->exec_alt[0] = st->exec;
+        st->graph_field_alt[0] = st->graph_field;
+        st->graph_merged_alt[0] = st->graph_merged;
+        st->graph_steps_alt[0] = st->graph_steps;
+        st->exec = nullptr;
+        st->graph_field = nullptr;
+        if (hit >= 0) {
+            st->exec = e;
+            st->graph_field = f;
+            st->graph_merged = m;
+            st->graph_steps = k;
         } else {
-            if (st->exec_alt) cudaGraphExecDestroy(st->exec_alt);
-            st->exec_alt = st->exec;
-            st->graph_field_alt = st->graph_field;
-            st->graph_merged_alt = st->graph_merged;
-            st->graph_steps_alt = st->graph_steps;
-            st->exec = nullptr;
             capture_graph(st, field, merged, 1);
         }
     }
@@ -1193,26 +1212,31 @@ int gp5cu_stepper_advance_host_many(gp5cu_stepper *st, int nstates, const void *
     use_device(p);
     if (nstates == 0) return GP5_OK;
     const size_t fb = p->field_bytes;
+    constexpr int NB = gp5cu_stepper::kHostStates;
+    // as many device states as there are host states, up to NB
+    const int nbuf = nstates < NB ? nstates : NB;
     if (!st->dstate) check_cuda(cudaMalloc(&st->dstate, fb), "cudaMalloc state");
-    if (!st->dstate2) check_cuda(cudaMalloc(&st->dstate2, fb), "cudaMalloc state");
+    for (int b = 1; b < nbuf; b++)
+        if (!st->dstate_more[b - 1]) check_cuda(cudaMalloc(&st->dstate_more[b - 1], fb), "cudaMalloc state");
     if (!st->up) {
         check_cuda(cudaStreamCreateWithFlags(&st->up, cudaStreamNonBlocking), "cudaStreamCreate");
         check_cuda(cudaStreamCreateWithFlags(&st->down, cudaStreamNonBlocking), "cudaStreamCreate");
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < NB; b++) {
             check_cuda(cudaEventCreateWithFlags(&st->ev_up[b], cudaEventDisableTiming), "cudaEventCreate");
             check_cuda(cudaEventCreateWithFlags(&st->ev_done[b], cudaEventDisableTiming), "cudaEventCreate");
             check_cuda(cudaEventCreateWithFlags(&st->ev_down[b], cudaEventDisableTiming), "cudaEventCreate");
         }
     }
-    void *dbuf[2] = {st->dstate, st->dstate2};
+    void *dbuf[NB] = {st->dstate};
+    for (int b = 1; b < NB; b++) dbuf[b] = st->dstate_more[b - 1];
     // the plan stream's earlier work (for example the last call's steps) comes first
     check_cuda(cudaEventRecord(st->ev_done[0], p->stream), "cudaEventRecord");
     check_cuda(cudaStreamWaitEvent(st->up, st->ev_done[0], 0), "cudaStreamWaitEvent");
     double t_after = st->t;
     for (int i = 0; i < nstates; i++) {
-        const int b = i & 1;
-        // buffer b is free once state i-2 has been downloaded from it
-        if (i >= 2) check_cuda(cudaStreamWaitEvent(st->up, st->ev_down[b], 0), "cudaStreamWaitEvent");
+        const int b = i % nbuf;
+        // buffer b is free once state i-nbuf has been downloaded from it
+        if (i >= nbuf) check_cuda(cudaStreamWaitEvent(st->up, st->ev_down[b], 0), "cudaStreamWaitEvent");
         check_cuda(cudaMemcpyAsync(dbuf[b], host_in[i], fb, cudaMemcpyHostToDevice, st->up), "upload");
         check_cuda(cudaEventRecord(st->ev_up[b], st->up), "cudaEventRecord");
         check_cuda(cudaStreamWaitEvent(p->stream, st->ev_up[b], 0), "cudaStreamWaitEvent");

@@ -145,17 +145,21 @@ struct gp5cu_stepper {
     void *graph_field = nullptr;
     bool graph_merged = false;
     int graph_steps = 0;
-    // the graph of the previously stepped field (two states alternate in the pipelined
-    // host-buffer entry point without re-capturing)
-    cudaGraphExec_t exec_alt = nullptr;
-    void *graph_field_alt = nullptr;
-    bool graph_merged_alt = false;
-    int graph_steps_alt = 0;
-    // pipelined host-buffer entry point: a second device state, upload / download streams and
-    // their events (created on first use)
-    void *dstate2 = nullptr;
+    // the graphs of the previously stepped fields, most recent first (the device states of
+    // the pipelined host-buffer entry point rotate without re-capturing)
+    static constexpr int kAltGraphs = 2;
+    cudaGraphExec_t exec_alt[kAltGraphs] = {};
+    void *graph_field_alt[kAltGraphs] = {};
+    bool graph_merged_alt[kAltGraphs] = {};
+    int graph_steps_alt[kAltGraphs] = {};
+    // pipelined host-buffer entry point: kHostStates device states in rotation (dstate is the
+    // first), upload / download streams and their events (created on first use).  A state's
+    // buffer is busy for its upload, its steps and its download; with three of them the
+    // uploads and downloads run back to back on the copy engines.
+    static constexpr int kHostStates = 3;
+    void *dstate_more[kHostStates - 1] = {};
     cudaStream_t up = nullptr, down = nullptr;
-    cudaEvent_t ev_up[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_down[2] = {nullptr, nullptr};
+    cudaEvent_t ev_up[kHostStates] = {}, ev_done[kHostStates] = {}, ev_down[kHostStates] = {};
     double t = 0;
     int launches_per_step = 0;
 };

@@ -190,9 +190,9 @@ int gp5cu_stepper_advance_host(gp5cu_stepper *st, const void *host_in, void *hos
                                int nsteps);
 /* The same for nstates independent host states (an ensemble, or states a caller streams
  * through the GPU): state i is uploaded from host_in[i], advanced nsteps steps and downloaded
- * to host_out[i].  Two device states alternate, with uploads and downloads on their own
+ * to host_out[i].  Three device states rotate, with uploads and downloads on their own
  * streams, so the upload of state i+1 and the download of state i-1 overlap the steps of
- * state i (pinned host buffers are needed for the copies to overlap).  host_in[i] and
+ * state i and each other (pinned host buffers are needed for the copies to overlap).  host_in[i] and
  * host_out[i] may alias; states that share an output buffer overwrite it in order.  The stepper's time
  * advances by nsteps steps once.  Single-solve plans only.  No reference counterpart (the
  * reference keeps one state per process). */

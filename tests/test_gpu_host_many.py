@@ -27,6 +27,10 @@ def test_host_many_matches_single_states(prec, imag):
         ref = np.empty_like(s)
         st.advance_host(s, ref, 3)
         assert np.array_equal(got, ref)
+    # fewer states than device states
+    two = [np.empty_like(s) for s in states[:2]]
+    st.advance_host_many(states[:2], two, 3)
+    assert all(np.array_equal(a, b) for a, b in zip(two, outs[:2]))
     # outputs may alias inputs
     same = [s.copy(order="F") for s in states[:3]]
     st.advance_host_many(same, same, 3)
