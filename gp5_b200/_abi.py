@@ -28,6 +28,7 @@ GP5_FORWARD, GP5_BACKWARD = -1, 1
 GP5_FUNC_GP, GP5_FUNC_LHY, GP5_FUNC_LHY_UNLOCKED = 0, 1, 2
 GP5_POT_NONE, GP5_POT_HARMONIC, GP5_POT_ARRAY = 0, 1, 2
 GP5_STEP_EULER, GP5_STEP_RK4 = 0, 1
+GP5_BATCH_RK4, GP5_BATCH_PRECOND = 0, 1
 
 
 class Gp5Error(RuntimeError):
@@ -146,6 +147,7 @@ def lib():
         "gp5cu_batch_get_state": (i, [vp, i, vp]),
         "gp5cu_batch_solve": (i, [vp, d, i, i, C.POINTER(SolveResult)]),
         "gp5cu_batch_launches": (C.c_longlong, [vp]),
+        "gp5cu_batch_set_method": (i, [vp, i, d]),
         "gp5cu_decompose": (i, [vp, vp, i, d, vp, C.POINTER(C.c_int)]),
         "gp5cu_decompose_host": (i, [vp, vp, i, d, vp, C.POINTER(C.c_int)]),
         "gp5cu_plan_autotune": (i, [vp]),
@@ -560,6 +562,11 @@ class Batch:
         out = np.empty((n, n, n, 1), dtype=np.complex128, order="F")
         check(lib().gp5cu_batch_get_state(self.h, k, C.c_void_p(_ptr(out))))
         return out
+
+    def set_method(self, method: int, theta: float = 0.5) -> None:
+        """GP5_BATCH_RK4 (imaginary-time RK4, the default) or GP5_BATCH_PRECOND (preconditioned
+        gradient iteration with step theta) for the following solve calls."""
+        check(lib().gp5cu_batch_set_method(self.h, int(method), float(theta)))
 
     def solve(self, tol: float, check_every: int = 100, max_steps: int = 100000):
         res = (SolveResult * len(self.solves))()

@@ -36,6 +36,9 @@ struct BatchGroup {
     void *psi = nullptr;  // idx.size() consecutive fields
     std::vector<DevScalars> ds_host;
     std::vector<DevScalars> st_host;  // the stepper's scalars (status of the bounded waits)
+    // graph of `pexec_iters` preconditioned iterations over `pexec_live` live solves
+    cudaGraphExec_t pexec = nullptr;
+    int pexec_iters = 0, pexec_live = 0;
 };
 
 struct gp5cu_batch {
@@ -48,6 +51,8 @@ struct gp5cu_batch {
     std::vector<int> group_of[2], slot_of[2];
     std::vector<char> in_c128;  // complex64 batch: the current state is the complex128 group's
     long long launches = 0;
+    int method = GP5_BATCH_RK4;  // gp5cu_batch_set_method
+    double theta = 0.5;
 };
 
 namespace {
@@ -61,6 +66,8 @@ void destroy_group(BatchGroup &g) {
         cudaSetDevice(g.plan->dev);
         cudaStreamSynchronize(g.plan->stream);
     }
+    if (g.pexec) cudaGraphExecDestroy(g.pexec);
+    g.pexec = nullptr;
     if (g.st) gp5cu_stepper_destroy(g.st);
     if (g.func) gp5cu_functional_destroy(g.func);
     if (g.psi) cudaFree(g.psi);
@@ -216,7 +223,47 @@ void convert_state(gp5cu_batch *b, int i, bool to128) {
     b->launches += 1;
 }
 
-// Imaginary-time RK4 of every solve of `groups` until done(i, residual, residual at the
+// Queues `iters` preconditioned iterations of every live solve of group g on its plan stream.
+void queue_precond(BatchGroup &g, int iters, double theta) {
+    dispatch_b(g.prec, [&](auto r) {
+        using Real = decltype(r);
+        for (int k = 0; k < iters; k++) Launch<Real>::precond_iter(g.func, g.st->sp, g.psi, g.st->Ka, theta);
+    });
+}
+
+// Captures `iters` preconditioned iterations of group g into g.pexec (after a configuring
+// pass that launches nothing, as for the step graphs).
+void build_precond_graph(BatchGroup &g, int iters, double theta) {
+    gp5cu_plan *p = g.plan;
+    if (g.pexec) cudaGraphExecDestroy(g.pexec);
+    g.pexec = nullptr;
+    p->dry = true;
+    try {
+        queue_precond(g, 1, theta);
+    } catch (...) {
+        p->dry = false;
+        throw;
+    }
+    p->dry = false;
+    cudaGraph_t gr = nullptr;
+    check_cuda(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        queue_precond(g, iters, theta);
+    } catch (...) {
+        cudaStreamEndCapture(p->stream, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        throw;
+    }
+    check_cuda(cudaStreamEndCapture(p->stream, &gr), "end capture");
+    const cudaError_t e = cudaGraphInstantiate(&g.pexec, gr, 0);
+    cudaGraphDestroy(gr);
+    check_cuda(e, "cudaGraphInstantiate");
+    g.pexec_iters = iters;
+    g.pexec_live = g.live;
+}
+
+// Imaginary-time RK4 (or, with GP5_BATCH_PRECOND, the preconditioned iteration) of every
+// solve of `groups` until done(i, residual, residual at the
 // previous check, steps taken in this phase) says so or the phase's step budget runs out;
 // results[i] holds the last check's observables.  Returns the steps of this phase per solve.
 template <class Done>
@@ -242,7 +289,14 @@ std::vector<int> run_phase(gp5cu_batch *b, int set, int check_every, const std::
             check_cuda(cudaSetDevice(p->dev), "cudaSetDevice");
             dispatch_b(g.prec, [&](auto r) {
                 using Real = decltype(r);
-                if (check > 0) {
+                if (check > 0 && b->method == GP5_BATCH_PRECOND) {
+                    // the check's reset scalars hold sigma = 1: the iterations read psi as stored
+                    if (!g.pexec || g.pexec_live != g.live || g.pexec_iters != chunk)
+                        build_precond_graph(g, chunk, b->theta);
+                    for (int k = 0; k < check_every; k += chunk)
+                        check_cuda(cudaGraphLaunch(g.pexec, p->stream), "cudaGraphLaunch");
+                    b->launches += (long long)check_every * Launch<Real>::kPrecondLaunches;
+                } else if (check > 0) {
                     if (!st->exec || st->graph_field != g.psi || st->graph_steps != chunk)
                         build_graph(st, g.psi, true, chunk);
                     set_scalars(p->stream, st->ds, p->nsolve);
@@ -274,7 +328,7 @@ std::vector<int> run_phase(gp5cu_batch *b, int set, int check_every, const std::
             int kept = 0;
             for (int q = 0; q < g.live; q++) {
                 const int i = g.idx[q];
-                if (check > 0 && (g.st_host[q].status & DS_TIMEOUT))
+                if (check > 0 && b->method == GP5_BATCH_RK4 && (g.st_host[q].status & DS_TIMEOUT))
                     fail(GP5_ERR_TIMEOUT, "a bounded device wait ran out (solve " + std::to_string(i) + ")");
                 if (check > 0) steps[i] += check_every;
                 const DevScalars &d = g.ds_host[q];
@@ -494,6 +548,25 @@ int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps
         results[i].steps_c64 = s32[i];
         results[i].converged = results[i].residual <= tol;
     }
+    GP5B_CATCH
+}
+
+int gp5cu_batch_set_method(gp5cu_batch *b, int method, double theta) {
+    GP5B_TRY
+    require_b(b != nullptr, "NULL argument");
+    require_b(method == GP5_BATCH_RK4 || method == GP5_BATCH_PRECOND, "method must be GP5_BATCH_RK4 or GP5_BATCH_PRECOND");
+    require_b(theta > 0 && theta <= 1, "theta must be in (0, 1]");
+    if (method != b->method || theta != b->theta)
+        for (auto &set : b->groups)
+            for (BatchGroup &g : set) {
+                if (g.pexec) {
+                    check_cuda(cudaSetDevice(g.plan->dev), "cudaSetDevice");
+                    cudaGraphExecDestroy(g.pexec);
+                }
+                g.pexec = nullptr;
+            }
+    b->method = method;
+    b->theta = theta;
     GP5B_CATCH
 }
 

@@ -472,6 +472,29 @@ void Launch<Real>::apply_h(gp5cu_functional *f, const void *src, void *dst, bool
     epilogue<Real>(p, P, obs);
 }
 
+// One preconditioned gradient iteration of every live solve of the plan (single component;
+// OpPrecondIn / OpPrecond / OpPrecondOut): H psi into hbuf with mu per solve, the residual's
+// transform with the shifted inverse kinetic operator in k-space, the update of psi with its
+// norm, then the normalisation.  sp_norm: parameters holding the target N and dV per solve.
+template <typename Real>
+void Launch<Real>::precond_iter(gp5cu_functional *f, const SolveParams *sp_norm, void *psi, void *hbuf,
+                                double theta) {
+    using V = cpx<Real>;
+    gp5cu_plan *p = f->plan;
+    apply_h(f, psi, hbuf, true);
+    OpPrecondIn<Real> in{(const V *)hbuf, (const V *)psi, (V *)p->work, p->ds, f->sp};
+    launch_axis<Real, true, MODE_FWD>(p, 0, in);
+    OpCopy<Real> cp{(const V *)p->work, (V *)p->work, p->nsolve > 1 ? f->sp : nullptr};
+    launch_axis<Real, false, MODE_FWD>(p, 1, cp);
+    OpPrecond<Real> pc{(const V *)p->work, (V *)p->work, f->sp, p->ds, p->shape[0], p->shape[1], p->shape[2],
+                       (double)p->nsites};
+    launch_axis<Real, false, MODE_FWD_MID_INV>(p, 2, pc);
+    launch_axis<Real, false, MODE_INV>(p, 1, cp);
+    OpPrecondOut<Real> out{(const V *)p->work, (V *)psi, p->ds, sp_norm, theta};
+    launch_axis<Real, true, MODE_INV>(p, 0, out);
+    scale(p, psi, 0, p->ds, false);
+}
+
 template <typename Real>
 void Launch<Real>::residual(gp5cu_plan *p, const void *psi, const void *hpsi, DevScalars *ds, const SolveParams *sp) {
     using V = cpx<Real>;

@@ -895,6 +895,131 @@ template <typename Real> struct OpResidual {
     __device__ __forceinline__ void finalize(const double *s, int solve) const { ds[solve].sums[5] = s[0]; }
 };
 
+// ---- preconditioned ground-state iteration ---------------------------------------------------
+// One iteration of every solve (single component):
+//   r = H psi - mu psi,  d = (alpha - 1/2m lap)^{-1} r,  psi <- (psi - theta d) normalised to N,
+// with mu = <psi|H psi>/<psi|psi> of the current state (ds[solve].mu, written by the observables
+// epilogue of the H application) and alpha = max(|mu|, kPrecondAlphaMin) per solve.  The inverse
+// of the kinetic operator shifted by alpha is applied in k-space, between a forward and an
+// inverse transform, so every Fourier mode of the residual moves at a rate of order one: the
+// iteration needs tens of passes where imaginary time needs thousands of steps, and its fixed
+// point (r = 0 at norm N) is the state imaginary-time evolution converges to.
+constexpr double kPrecondAlphaMin = 0.05;
+
+// x forward pass: the transform input is the residual H psi - mu psi
+template <typename Real> struct OpPrecondIn {
+    static constexpr int NRED = 0, BATCH = 1;
+    using Ctx = SolveCtx;
+    using V = cpx<Real>;
+    using Pre = NoPre;
+    const V *hpsi, *psi;
+    V *dst;
+    const DevScalars *ds;
+    const SolveParams *sp;
+    __device__ __forceinline__ const SolveParams *params() const { return sp; }
+    __device__ __forceinline__ const DevScalars *scalars() const { return nullptr; }
+    __device__ __forceinline__ V load(V h, long long g, const LineRef &e, double *, const SolveCtx &) const {
+        const Real mu = (Real)__ldg(&ds[e.solve].mu);
+        return csub(h, cscale(psi[g], mu));
+    }
+    __device__ __forceinline__ V mid(V v, const LineRef &, const SolveCtx &) const { return v; }
+    __device__ __forceinline__ Pre pre(long long) const { return Pre{}; }
+    __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &, double *, const SolveCtx &) const {
+        dst[g] = v;
+    }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const {
+        p[0] = hpsi;
+        p[1] = psi;
+        return 2;
+    }
+    __device__ __forceinline__ void finalize(const double *, int) const {}
+};
+
+// z pass: forward z, times 1 / (ns (alpha + kin ns K^2)), inverse z.  kin = 1/(2 m ns) is the
+// plan's kinetic multiplier, so kin ns K^2 = K^2 / 2m, and the 1/ns is the normalisation of
+// the unnormalised inverse transform.  The factor is formed in FP64 in both precisions.
+template <typename Real> struct OpPrecond {
+    static constexpr int NRED = 0, BATCH = 1;
+    using Ctx = SolveCtx;
+    using V = cpx<Real>;
+    using Pre = NoPre;
+    const V *src;
+    V *dst;
+    const SolveParams *sp;
+    const DevScalars *ds;
+    int nx, ny, nz;
+    double ns;  // sites per solve
+    __device__ __forceinline__ const SolveParams *params() const { return sp; }
+    __device__ __forceinline__ const DevScalars *scalars() const { return nullptr; }
+    __device__ __forceinline__ double alpha(int solve) const {
+        return fmax(fabs(__ldg(&ds[solve].mu)), kPrecondAlphaMin);
+    }
+    __device__ __forceinline__ V load(V x, long long, const LineRef &, double *, const SolveCtx &) const { return x; }
+    __device__ __forceinline__ V mid(V v, const LineRef &e, const SolveCtx &X) const {
+        const SolveParams &S = X.S;
+        const double kx = momentum(S, 0, e.i, nx), ky = momentum(S, 1, e.j, ny), kz = momentum(S, 2, e.k, nz);
+        const double k2 = (kx * kx + ky * ky) + kz * kz;
+        return cscale(v, (Real)(1.0 / (ns * alpha(e.solve) + S.kin[e.c] * ns * ns * k2)));
+    }
+    static constexpr bool MID_Z = true;
+    struct MidLine {
+        double kxy2, dkz, a, b;
+    };
+    __device__ __forceinline__ MidLine mid_line(const LineRef &e, const SolveCtx &X) const {
+        const SolveParams &S = X.S;
+        const double kx = momentum(S, 0, e.i, nx), ky = momentum(S, 1, e.j, ny);
+        return MidLine{kx * kx + ky * ky, S.dk[2], ns * alpha(e.solve), S.kin[e.c] * ns * ns};
+    }
+    __device__ __forceinline__ V mid_z(V v, int kidx, const MidLine &L) const {
+        const double kz = L.dkz * (double)kidx;
+        return cscale(v, (Real)(1.0 / (L.a + L.b * (L.kxy2 + kz * kz))));
+    }
+    __device__ __forceinline__ Pre pre(long long) const { return Pre{}; }
+    __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &, double *, const SolveCtx &) const {
+        dst[g] = v;
+    }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const { p[0] = src; return 1; }
+    __device__ __forceinline__ void finalize(const double *, int) const {}
+};
+
+// x inverse pass: psi <- psi - theta d, with sum |psi|^2 per solve -> the normalisation factor
+// sqrt(N / (dV S)) in ds[solve].factor (applied by an OpScale pass)
+template <typename Real> struct OpPrecondOut {
+    static constexpr int NRED = 1, BATCH = 4;
+    using Ctx = SolveCtx;
+    using V = cpx<Real>;
+    struct Pre {
+        V p;
+    };
+    const V *src;  // transform buffer
+    V *psi;
+    DevScalars *ds;
+    const SolveParams *sp;  // targets N and cell volumes
+    double theta;
+    __device__ __forceinline__ const SolveParams *params() const { return sp; }
+    __device__ __forceinline__ const DevScalars *scalars() const { return nullptr; }
+    __device__ __forceinline__ V load(V x, long long, const LineRef &, double *, const SolveCtx &) const { return x; }
+    __device__ __forceinline__ V mid(V v, const LineRef &, const SolveCtx &) const { return v; }
+    __device__ __forceinline__ Pre pre(long long g) const { return Pre{psi[g]}; }
+    __device__ __forceinline__ void post(long long g, const LineRef &, V v, const Pre &q, double *acc,
+                                         const SolveCtx &) const {
+        const V r = csub(q.p, cscale(v, (Real)theta));
+        psi[g] = r;
+        acc[0] += (double)r.x * (double)r.x + (double)r.y * (double)r.y;
+    }
+    __device__ __forceinline__ int streams(const void *(&p)[4]) const {
+        p[0] = src;
+        p[1] = psi;
+        return 2;
+    }
+    __device__ __forceinline__ void finalize(const double *s, int solve) const {
+        const SolveParams &S = sp[solve];
+        DevScalars &d = ds[solve];
+        d.factor = sqrt(S.Nt[0] / (S.dV * s[0]));
+        if (!isfinite(s[0]) || !isfinite(d.factor)) d.status |= DS_NONFINITE;
+    }
+};
+
 // complex128 <-> plan precision conversion over nsites elements (one solve)
 template <typename Real> struct OpConvert {
     static constexpr int NRED = 0;

@@ -187,6 +187,9 @@ template <typename Real> struct Launch {
     static void prologue(gp5cu_stepper *st, void *field);  // forward x transform of psi
     static void phase_exp(gp5cu_plan *p, const void *phase, void *out);
     static void init_gaussian(gp5cu_plan *p, void *field, int comp, const double sigma[3]);
+    // one preconditioned gradient iteration of every solve (ground states, single component)
+    static void precond_iter(gp5cu_functional *f, const SolveParams *sp_norm, void *psi, void *hbuf, double theta);
+    static constexpr int kPrecondLaunches = 11;
     // times every tile shape (and, with radix, both radix schedules) of the strided y/z passes
     // on the zeroed work field, and with radix both schedules of the stage boundary; keeps the
     // fastest in p->tile_threads, p->radix and p->radix_boundary

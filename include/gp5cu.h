@@ -266,6 +266,20 @@ int gp5cu_batch_get_state(gp5cu_batch *b, int solve, double *host_c128);
  * or max_steps; results[i] per solve.  Returns GP5_OK even if some solves did not converge. */
 int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps,
                       gp5cu_solve_result *results);
+/* Method of the following gp5cu_batch_solve calls.  No reference counterpart (the reference
+ * reaches ground states only by imaginary-time stepping).
+ * GP5_BATCH_RK4 (the default): renormalised imaginary-time RK4 with each solve's dt.
+ * GP5_BATCH_PRECOND: preconditioned gradient iteration towards the same ground state,
+ *   psi <- normalise_N(psi - theta (alpha - 1/2 lap)^{-1} (H psi - mu psi)),
+ * mu = <psi|H psi>/<psi|psi> and alpha = max(|mu|, 0.05) per solve, the shifted inverse kinetic
+ * operator applied in k-space; its fixed point (zero residual at norm N) is the one imaginary
+ * time converges to, and it takes tens of iterations where imaginary time takes thousands of
+ * steps (each iteration costs about half an RK4 step: eleven launches).  The dt of the solve
+ * descriptors is not used; gp5cu_solve_result.steps counts iterations.  theta in (0, 1]; 0.5
+ * converges on the droplets of N in [20, 2000], c3 in [-3.2, -2.8]. */
+#define GP5_BATCH_RK4 0
+#define GP5_BATCH_PRECOND 1
+int gp5cu_batch_set_method(gp5cu_batch *b, int method, double theta);
 /* Kernel launches of the last gp5cu_batch_solve call. */
 long long gp5cu_batch_launches(const gp5cu_batch *b);
 

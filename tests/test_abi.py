@@ -59,6 +59,8 @@ def test_new_entry_points_reject_bad_arguments_without_device():
     assert L.gp5cu_stepper_set_compensation(None, 1) == _abi.GP5_ERR_ARG
     assert L.gp5cu_mlp_forward(None, None, 1, None) == _abi.GP5_ERR_ARG
     assert L.gp5cu_gemm_bf16(None, 1, 1, None, 1, 1, None, 1, 1, 1, 1, None) == _abi.GP5_ERR_ARG
+    assert L.gp5cu_batch_set_method(None, _abi.GP5_BATCH_PRECOND, 0.5) == _abi.GP5_ERR_ARG
+    assert L.gp5cu_init_gaussian(None, None, 0, None) == _abi.GP5_ERR_ARG
 
 
 def test_reference_facing_bindings_expose_the_extensions():

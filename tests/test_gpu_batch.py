@@ -128,3 +128,37 @@ def test_complex64_batch_converges_to_residual_like_complex128():
         assert 0 < a["steps_c64"] <= a["steps"]
         assert abs(a["energy"] - c["energy"]) <= 1e-9 * abs(c["energy"])
         assert abs(a["mu"] - c["mu"]) <= 1e-8 * abs(c["mu"])
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_preconditioned_batch_reaches_the_imaginary_time_ground_states(prec):
+    """GP5_BATCH_PRECOND reaches the states that imaginary-time RK4 converges to (energy, mu
+    and |psi|) in tens of iterations, where RK4 takes thousands of steps; a complex64 batch runs
+    its bulk in complex64 and finishes in complex128.  The converged observables agree with the
+    oracle's evaluation of the returned state."""
+    from gp5_b200 import _abi as abi
+    brk, rrk, starts = _converged_batch(abi.GP5_C128)
+    b = abi.Batch(CONVERGE, precision=prec)
+    b.set_method(abi.GP5_BATCH_PRECOND, 0.5)
+    for k, psi in enumerate(starts):
+        b.set_state(k, psi)
+    res = b.solve(tol=1e-8, check_every=5, max_steps=2000)
+    for k, (r, c, sd) in enumerate(zip(res, rrk, CONVERGE)):
+        assert r["converged"] and r["residual"] <= 1e-8, r
+        assert r["steps"] <= 200 and r["steps"] * 10 < c["steps"], (r["steps"], c["steps"])
+        assert (r["steps_c64"] > 0) == (prec == 1)
+        assert abs(r["energy"] - c["energy"]) <= 1e-9 * abs(c["energy"])
+        # mu moves to first order with the state (the energy to second order): at residual
+        # 1e-8 both solvers' states differ by about residual / gap
+        assert abs(r["mu"] - c["mu"]) <= 1e-6 * abs(c["mu"])
+        got = b.get_state(k)
+        a = np.abs(brk.get_state(k))
+        assert np.max(np.abs(np.abs(got) - a)) <= 1e-5 * np.max(a)
+        geo = o.Geometry((sd["n"],) * 3, (-sd["L"] / 2,) * 3, (sd["L"] / 2,) * 3)
+        ob = o.observables(o.Functional("lhy", c3=sd["c3"]), got, geo)
+        assert abs(ob["E"] - r["energy"]) <= 1e-10 * abs(ob["E"])
+        assert abs(ob["norm"] - sd["N"]) <= 1e-9 * sd["N"]
+    with pytest.raises(abi.Gp5Error):
+        b.set_method(abi.GP5_BATCH_PRECOND, 1.5)
+    with pytest.raises(abi.Gp5Error):
+        b.set_method(7, 0.5)
