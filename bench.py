@@ -724,6 +724,33 @@ def cpu_ground_state_baseline(gs: dict, seconds_per_grid: float = 4.0):
                       f"({sum(gs['_steps'])} steps in total, {total:.0f} s on the host)"}
 
 
+def cpu_precond_baseline(gp: dict, iters: int = 10):
+    """Ground states/s of the oracle's preconditioned iteration (oracle.gp_oracle.
+    precond_ground_state: the same method in FP64 numpy, all host threads) on the same droplets,
+    extrapolated like cpu_ground_state_baseline: the time of `iters` iterations (with a residual
+    check every 5, as on the GPU) per grid size, charged with the GPU's iteration count of every
+    solve."""
+    import numpy as np
+
+    from oracle import gp_oracle as o
+
+    o.set_elementwise_threads(o._WORKERS)
+    per_iter = {}
+    for n in sorted(set(gp["_grids"])):
+        sd = next(s for s in batch_solves(len(gp["_grids"])) if s["n"] == n)
+        geo = o.Geometry((n,) * 3, (-sd["L"] / 2,) * 3, (sd["L"] / 2,) * 3)
+        psi = np.asfortranarray(droplet_state(sd, 1)[..., None])
+        func = o.Functional("lhy", c3=sd["c3"], c4=sd["c4"])
+        t0 = time.perf_counter()
+        o.precond_ground_state(func, geo, psi, sd["N"], tol=0.0, check_every=5, max_iter=iters)
+        per_iter[n] = (time.perf_counter() - t0) / iters
+    total = sum(k * per_iter[n] for k, n in zip(gp["_steps"], gp["_grids"]))
+    return {"value": len(gp["_steps"]) / total, "unit": "ground states/s", "cores": o._WORKERS, "kind": "port",
+            "seconds_per_iteration": {str(n): t for n, t in per_iter.items()},
+            "sample": f"{iters} iterations per grid size; extrapolated to the GPU solver's iteration count of "
+                      f"every solve ({sum(gp['_steps'])} in total, {total:.0f} s on the host)"}
+
+
 def cpu_reference_timing(max_seconds: float, max_steps: int, warmup: int = 1):
     """RK4 steps of the oracle (the reference's arithmetic) on the host, all threads: `warmup`
     untimed steps, then up to `max_steps` timed steps or `max_seconds`, whichever ends first."""
@@ -877,6 +904,7 @@ def main():
     if gs is not None:
         if world == 1 and not args.no_cpu_baseline:
             gs["cpu_baseline"] = cpu_ground_state_baseline(gs)
+            gs["preconditioned"]["cpu_baseline"] = cpu_precond_baseline(gs["preconditioned"])
         e128 = gs.pop("energies_rank0")
         e64 = gs["c64"].pop("energies_rank0")
         gs["c64"]["max_energy_rel_diff_vs_c128"] = max(abs(a - b) / abs(b) for a, b in zip(e64, e128))
