@@ -899,12 +899,14 @@ template <typename Real> struct OpResidual {
 // One iteration of every solve (single component):
 //   r = H psi - mu psi,  d = (alpha - 1/2m lap)^{-1} r,  psi <- (psi - theta d) normalised to N,
 // with mu = <psi|H psi>/<psi|psi> of the current state (ds[solve].mu, written by the observables
-// epilogue of the H application) and alpha = max(|mu|, kPrecondAlphaMin) per solve.  The inverse
+// epilogue of the H application) and alpha = max(|mu|, kPrecondAlphaMin, kPrecondVShare Vmax)
+// per solve, Vmax the harmonic potential at the farthest cell centre (the preconditioner does
+// not see V: theta (V - mu) / alpha must stay below 2 where V is large).  The inverse
 // of the kinetic operator shifted by alpha is applied in k-space, between a forward and an
 // inverse transform, so every Fourier mode of the residual moves at a rate of order one: the
 // iteration needs tens of passes where imaginary time needs thousands of steps, and its fixed
 // point (r = 0 at norm N) is the state imaginary-time evolution converges to.
-constexpr double kPrecondAlphaMin = 0.05;
+constexpr double kPrecondAlphaMin = 0.05, kPrecondVShare = 0.5;
 
 // x forward pass: the transform input is the residual H psi - mu psi
 template <typename Real> struct OpPrecondIn {
@@ -951,15 +953,21 @@ template <typename Real> struct OpPrecond {
     double ns;  // sites per solve
     __device__ __forceinline__ const SolveParams *params() const { return sp; }
     __device__ __forceinline__ const DevScalars *scalars() const { return nullptr; }
-    __device__ __forceinline__ double alpha(int solve) const {
-        return fmax(fabs(__ldg(&ds[solve].mu)), kPrecondAlphaMin);
+    __device__ __forceinline__ double alpha(int solve, const SolveParams &S) const {
+        const int n[3] = {nx, ny, nz};
+        double vmax = 0.0;
+        for (int d = 0; d < 3; d++) {
+            const double lo = S.left[d] + 0.5 * S.dx[d], hi = S.left[d] + (n[d] - 0.5) * S.dx[d];
+            vmax += S.om2[0][d] * fmax(lo * lo, hi * hi);
+        }
+        return fmax(fmax(fabs(__ldg(&ds[solve].mu)), kPrecondAlphaMin), kPrecondVShare * 0.5 * vmax);
     }
     __device__ __forceinline__ V load(V x, long long, const LineRef &, double *, const SolveCtx &) const { return x; }
     __device__ __forceinline__ V mid(V v, const LineRef &e, const SolveCtx &X) const {
         const SolveParams &S = X.S;
         const double kx = momentum(S, 0, e.i, nx), ky = momentum(S, 1, e.j, ny), kz = momentum(S, 2, e.k, nz);
         const double k2 = (kx * kx + ky * ky) + kz * kz;
-        return cscale(v, (Real)(1.0 / (ns * alpha(e.solve) + S.kin[e.c] * ns * ns * k2)));
+        return cscale(v, (Real)(1.0 / (ns * alpha(e.solve, S) + S.kin[e.c] * ns * ns * k2)));
     }
     static constexpr bool MID_Z = true;
     struct MidLine {
@@ -968,7 +976,7 @@ template <typename Real> struct OpPrecond {
     __device__ __forceinline__ MidLine mid_line(const LineRef &e, const SolveCtx &X) const {
         const SolveParams &S = X.S;
         const double kx = momentum(S, 0, e.i, nx), ky = momentum(S, 1, e.j, ny);
-        return MidLine{kx * kx + ky * ky, S.dk[2], ns * alpha(e.solve), S.kin[e.c] * ns * ns};
+        return MidLine{kx * kx + ky * ky, S.dk[2], ns * alpha(e.solve, S), S.kin[e.c] * ns * ns};
     }
     __device__ __forceinline__ V mid_z(V v, int kidx, const MidLine &L) const {
         const double kz = L.dkz * (double)kidx;

@@ -271,7 +271,8 @@ int gp5cu_batch_solve(gp5cu_batch *b, double tol, int check_every, int max_steps
  * GP5_BATCH_RK4 (the default): renormalised imaginary-time RK4 with each solve's dt.
  * GP5_BATCH_PRECOND: preconditioned gradient iteration towards the same ground state,
  *   psi <- normalise_N(psi - theta (alpha - 1/2 lap)^{-1} (H psi - mu psi)),
- * mu = <psi|H psi>/<psi|psi> and alpha = max(|mu|, 0.05) per solve, the shifted inverse kinetic
+ * mu = <psi|H psi>/<psi|psi> and alpha = max(|mu|, 0.05, Vmax/2) per solve (Vmax: the trap's
+ * potential at the farthest cell centre, 0 without a trap), the shifted inverse kinetic
  * operator applied in k-space; its fixed point (zero residual at norm N) is the one imaginary
  * time converges to, and it takes tens of iterations where imaginary time takes thousands of
  * steps (each iteration costs about half an RK4 step: eleven launches).  The dt of the solve

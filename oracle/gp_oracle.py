@@ -477,13 +477,17 @@ def lhy_mu_protocol(shape=(30, 30, 30), box=10.0, sigma=5.0, N=370.0, dt_factor=
 # --------------------------------------------------------------------------------------
 def precond_ground_state(func: "Functional", geo: Geometry, psi: np.ndarray, N: float, theta: float = 0.5,
                          tol: float = 1e-8, check_every: int = 5, max_iter: int = 2000,
-                         alpha_min: float = 0.05):
+                         alpha_min: float = 0.05, v_share: float = 0.5):
     """psi <- normalise_N(psi - theta (alpha - 1/2 lap)^{-1} (H psi - mu psi)) until the residual
     ||H psi - mu psi|| / ||psi|| (observables) is at most tol, checked every check_every
-    iterations; mu = Re<psi|H psi>/<psi|psi> and alpha = max(|mu|, alpha_min) of the current
-    state, the shifted inverse kinetic operator (unit mass, one component) applied in k-space.
-    The same arithmetic as the batched solver's GP5_BATCH_PRECOND.  Returns (psi, iterations,
-    observables of the last check)."""
+    iterations; mu = Re<psi|H psi>/<psi|psi> of the current state and alpha = max(|mu|,
+    alpha_min, v_share max V), the shifted inverse kinetic operator (unit mass, one component)
+    applied in k-space.  The preconditioner does not see the external potential V: a shift well
+    below its maximum lets the slowly varying modes where V is large overshoot (theta (V - mu) /
+    alpha must stay below 2), so the shift takes a share of max V over the grid (0 without a
+    potential).  The same arithmetic as the batched solver's GP5_BATCH_PRECOND.  Returns (psi,
+    iterations, observables of the last check)."""
+    vcap = v_share * float(np.max(func.V)) if func.V is not None else 0.0
     psi = np.array(psi, dtype=np.complex128, order="F")
     half_k2 = 0.5 * k2_tensor(geo)
     it = 0
@@ -495,7 +499,7 @@ def precond_ground_state(func: "Functional", geo: Geometry, psi: np.ndarray, N: 
         h = func.apply(psi, geo)
         mu = float(np.sum((np.conj(psi) * h).real)) / float(np.sum(np.abs(psi) ** 2))
         r = (h - mu * psi)[..., 0]
-        d = np.fft.ifftn(np.fft.fftn(r) / (max(abs(mu), alpha_min) + half_k2))
+        d = np.fft.ifftn(np.fft.fftn(r) / (max(abs(mu), alpha_min, vcap) + half_k2))
         psi[..., 0] = psi[..., 0] - theta * d
         normalize(N, psi, 0, geo)
         it += 1

@@ -24,3 +24,19 @@ def test_preconditioned_iteration_reaches_an_imaginary_time_fixed_point(N, c3, n
     ob2 = o.observables(func, psi2, geo)
     assert abs(ob2["E"] - ob["E"]) <= 1e-10 * abs(ob["E"])
     assert np.max(np.abs(np.abs(psi2) - np.abs(psi))) <= 1e-6 * np.max(np.abs(psi))
+
+
+@pytest.mark.parametrize("N,c3,omega,n", [(20.0, -3.0, 0.1, 32), (200.0, -2.9, 0.1, 32)])
+def test_preconditioned_iteration_converges_in_a_trap(N, c3, omega, n):
+    """With a harmonic trap the shift takes half the potential's maximum: without it the slowly
+    varying modes at the box corners overshoot and the iteration diverges for large boxes."""
+    L = 4.0 * N ** (1.0 / 3.0)
+    geo = o.Geometry((n,) * 3, (-L / 2,) * 3, (L / 2,) * 3)
+    psi0 = o.gaussian_with_noise(geo, 0.5 * N ** (1.0 / 3.0), 1e-3, seed=5, N=N, phase_noise=True)
+    func = o.Functional("lhy", c3=c3, V=o.harmonic_potential(geo, [(omega,) * 3]))
+    psi, it, ob = o.precond_ground_state(func, geo, psi0, N, max_iter=400)
+    assert ob["residual"] <= 1e-8, (it, ob["residual"])
+    dx = L / n
+    st = o.Stepper(func, geo, 0.15 * dx * dx, normalizations=[N])
+    ob2 = o.observables(func, st.advance(psi.copy(), 50), geo)
+    assert abs(ob2["E"] - ob["E"]) <= 1e-10 * abs(ob["E"])
