@@ -320,10 +320,13 @@ class WarmStart:
 def solve_ground_states(params: Sequence[dict], grid, tol: float, chunk: int = 512,
                         check_every: int = 100, max_steps: int = 400000, precision: int = _abi.GP5_C128,
                         starts=None, device: int = 0, seed: int = 0, keep=None, progress=None,
-                        devices: Optional[Sequence[int]] = None):
+                        devices: Optional[Sequence[int]] = None, method: int = _abi.GP5_BATCH_RK4):
     """Solves every parameter set with the batched solver from a Gaussian (or
     starts(p, n, index)) on grid(p) (an int or a function of p); returns (states, results)
     lists in the order of params, each state passed through keep(p, psi) when keep is given.
+    method: GP5_BATCH_RK4 (imaginary time; results count RK4 steps) or GP5_BATCH_PRECOND (the
+    preconditioned iteration to the same ground states, with its step 0.5; results count
+    iterations).
 
     The solves go to the batched solver `chunk` at a time (gp5cu_batch_*), which takes
     finished solves out of its launches at every convergence check, so slow solves cost only
@@ -341,6 +344,8 @@ def solve_ground_states(params: Sequence[dict], grid, tol: float, chunk: int = 5
             progress(c0, count)
         b = _abi.Batch([descs[i] for i in part], precision=precision, devices=devs)
         try:
+            if method != _abi.GP5_BATCH_RK4:
+                b.set_method(method, 0.5)
             for k, i in enumerate(part):
                 if starts is not None:
                     psi = starts(params[i], descs[i]["n"], i)
@@ -369,13 +374,15 @@ def training_grid(p: dict) -> int:
 def make_training_set(count: int = 4096, seed: int = TRAIN_SEED, grid=training_grid, tol: float = 1e-7,
                       chunk: int = 1024, device: int = 0, devices: Optional[Sequence[int]] = None,
                       targets: str = "axis", start_model: Optional["WarmStart"] = None, workers: int = 8,
-                      precision: int = _abi.GP5_C128):
+                      precision: int = _abi.GP5_C128, method: int = _abi.GP5_BATCH_RK4):
     """Ground states of `count` seeded parameter sets (batched imaginary-time RK4 from the
     noise-free Gaussian, or from start_model's prediction, to residual tol, on grid(p)^3),
     spread over `devices` when given; returns (params, samples [count][64], solver results).
 
     targets "axis": the states' axis samples (radial_samples); "lsq": the least-squares
-    samples (lsq_samples), fitted after each chunk of solves by `workers` spawned processes."""
+    samples (lsq_samples), fitted after each chunk of solves by `workers` spawned processes.
+    method: the batched solver's method (GP5_BATCH_PRECOND reaches the same ground states in
+    tens of iterations instead of thousands of RK4 steps)."""
     params = sample_params(count, seed)
     import sys
     import time
@@ -391,7 +398,8 @@ def make_training_set(count: int = 4096, seed: int = TRAIN_SEED, grid=training_g
         keep = lambda p, psi: radial_samples(psi, p["N"])
         samples, results = solve_ground_states(params, grid, tol=tol, chunk=chunk, device=device, keep=keep,
                                                progress=report, devices=devices, starts=starts,
-                                               precision=precision)
+                                               precision=precision, method=method,
+                                               check_every=5 if method == _abi.GP5_BATCH_PRECOND else 100)
         return params, np.asarray(samples), results
     if targets != "lsq":
         raise ValueError("targets must be 'axis' or 'lsq'")
@@ -407,7 +415,8 @@ def make_training_set(count: int = 4096, seed: int = TRAIN_SEED, grid=training_g
             keep = lambda p, psi: np.abs(psi).astype(np.float32)
             st, rs = solve_ground_states([params[i] for i in part], grid, tol=tol, chunk=len(part),
                                          device=device, keep=keep, devices=devices, precision=precision,
-                                         starts=lambda p, n, k: starts(p, n, k))
+                                         starts=lambda p, n, k: starts(p, n, k), method=method,
+                                         check_every=5 if method == _abi.GP5_BATCH_PRECOND else 100)
             fits = pool.map(_lsq_job, [(st[k], params[i]["N"]) for k, i in enumerate(part)])
             for k, i in enumerate(part):
                 samples[i], results[i] = fits[k], rs[k]
@@ -485,6 +494,9 @@ def main(argv=None):
     ap.add_argument("--workers", type=int, default=8, help="processes fitting least-squares targets")
     ap.add_argument("--complex64", action="store_true",
                     help="training solves with the complex64 bulk and complex128 polish")
+    ap.add_argument("--solver", choices=["rk4", "precond"], default="rk4",
+                    help="training solves by imaginary-time RK4 or by the preconditioned iteration "
+                         "(the same ground states, tens of iterations per solve)")
     a = ap.parse_args(argv)
     if a.train:
         t0 = time.time()
@@ -498,7 +510,8 @@ def main(argv=None):
             params, samples, results = make_training_set(
                 a.count, grid=grid, devices=a.devices, targets=a.targets, start_model=start_model,
                 chunk=a.chunk, workers=a.workers,
-                precision=_abi.GP5_C64 if a.complex64 else _abi.GP5_C128)
+                precision=_abi.GP5_C64 if a.complex64 else _abi.GP5_C128,
+                method=_abi.GP5_BATCH_PRECOND if a.solver == "precond" else _abi.GP5_BATCH_RK4)
             if start_model is not None:
                 start_model.close()
             steps = np.array([r["steps"] for r in results])
