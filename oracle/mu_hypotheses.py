@@ -13,6 +13,9 @@ per variant:
   grid=32       a 32^3 grid on the same box
   euler         the Euler stepper instead of RK4
   spb=100       100-step blocks (the stepsPerBlock of python/test/test.py:172)
+  spacing29     the spacing L/(n - 1) (box widened to +-10*30/29)
+  exact         the discrete ground state's mu = <psi|H psi>/N (preconditioned iteration to
+                residual 1e-12): the dt -> 0 limit of the protocol
   permuted      the data with its axes permuted (y, z, x): the P3DFFT path with
                 fftOrdering [2,0,1] (gp.py:35-38) only permutes the k-space axes, and on this
                 cubic grid and box it must reproduce 'restated' to rounding
@@ -85,6 +88,17 @@ def run(name: str):
         mu, it, _ = o.lhy_mu_protocol(shape=(n,) * 3)
     elif name.startswith("spb="):
         mu, it, _ = o.lhy_mu_protocol(steps_per_block=int(name[4:]))
+    elif name == "spacing29":
+        # the spacing L/(n - 1) of a vertex-based grid: the box widened to +-10*30/29
+        mu, it, _ = o.lhy_mu_protocol(box=10.0 * 30 / 29)
+    elif name == "exact":
+        # the discrete ground state itself (no time step): mu = <psi|H psi>/N at residual 1e-12
+        geo = o.Geometry((30,) * 3, (-10.0,) * 3, (10.0,) * 3)
+        psi = o.new_field(geo)
+        o.init_gaussian(geo, 5.0, psi)
+        o.normalize(370.0, psi, 0, geo)
+        _, it, ob = o.precond_ground_state(o.Functional("lhy"), geo, psi, 370.0, tol=1e-12, max_iter=5000)
+        mu = ob["mu"]
     elif name == "euler":
         mu, it = _protocol_euler()
     elif name == "permuted":
@@ -95,7 +109,7 @@ def run(name: str):
 
 
 VARIANTS = ["restated", "dt=0.001", "dt=0.002", "dt=0.004", f"dt={0.02 * (20.0 / 30) ** 2!r}", "N=371", "grid=32",
-            "euler", "spb=100", "permuted"]
+            "euler", "spb=100", "permuted", "spacing29", f"dt={0.01 * (20.0 / 29) ** 2!r}", "exact"]
 
 if __name__ == "__main__":
     for v in sys.argv[1:] or VARIANTS:
