@@ -11,6 +11,7 @@ class FakeBatch:
     """Stands in for _abi.Batch: solve i converges after need[i] steps in total."""
     need = {}
     created = []
+    methods = []
 
     def __init__(self, descs, precision=0, device=0, devices=None):
         self.descs = descs
@@ -34,6 +35,9 @@ class FakeBatch:
                             energy=-key, mu=-1.0, norm=key))
         return out
 
+    def set_method(self, method, theta=0.5):
+        FakeBatch.methods.append((method, theta))
+
     def get_state(self, k):
         return self.states[k][..., None]
 
@@ -55,6 +59,23 @@ def test_chunks_count_steps_and_keep_order(monkeypatch):
     assert all(r["converged"] for r in res)
     assert [r["energy"] for r in res] == [-p["N"] for p in params]
     assert FakeBatch.created == [3, 3, 1]
+
+
+def test_preconditioned_method_reaches_every_chunk(monkeypatch):
+    """method=GP5_BATCH_PRECOND is set on every chunk's batch with the step 0.5; the default
+    leaves the batches on imaginary-time RK4."""
+    params = [dict(N=float(30 + k), c3=-3.0, omega=0.0) for k in range(5)]
+    FakeBatch.need = {p["N"]: 40 for p in params}
+    FakeBatch.created, FakeBatch.methods = [], []
+    monkeypatch.setattr(ws._abi, "Batch", FakeBatch)
+    starts = lambda p, n, i: np.zeros((4, 4, 4), complex)
+    _, res = ws.solve_ground_states(params, 4, tol=1e-8, chunk=2, starts=starts, check_every=5,
+                                    method=ws._abi.GP5_BATCH_PRECOND)
+    assert FakeBatch.methods == [(ws._abi.GP5_BATCH_PRECOND, 0.5)] * 3
+    assert [r["steps"] for r in res] == [40] * 5
+    FakeBatch.methods = []
+    ws.solve_ground_states(params, 4, tol=1e-8, chunk=2, starts=starts)
+    assert FakeBatch.methods == []
 
 
 def test_unconverged_at_max_steps(monkeypatch):
