@@ -60,3 +60,17 @@ def test_roofline_of_a_step_with_l2_slabs():
     assert rf["kernel"] == "x_stage_boundary"
     assert rf["step"]["algorithmic_bytes"] == pytest.approx(31 * F)
     assert rf["per_kind_ms"]["z_fwd_kinetic_inv"] == pytest.approx(16 * 0.03)
+
+
+def test_cpu_baseline_of_the_preconditioned_leg(monkeypatch):
+    """The oracle's preconditioned iteration is timed per iteration at each grid size of the
+    leg and charged with the GPU's iteration count of every solve."""
+    small = [dict(n=16, L=12.0, N=30.0, c3=-3.0, c4=2.5, omega=0.0, dt=0.0),
+             dict(n=24, L=16.0, N=60.0, c3=-3.1, c4=2.5, omega=0.0, dt=0.0)]
+    monkeypatch.setattr(bench, "batch_solves", lambda count, seed=2025, rank=0: small)
+    gp = {"_steps": [40, 55], "_grids": [16, 24]}
+    r = bench.cpu_precond_baseline(gp, iters=2)
+    per = r["seconds_per_iteration"]
+    assert set(per) == {"16", "24"} and all(t > 0 for t in per.values())
+    assert r["value"] == pytest.approx(2 / (40 * per["16"] + 55 * per["24"]))
+    assert r["unit"] == "ground states/s" and r["kind"] == "port" and r["cores"] >= 1
